@@ -1,0 +1,102 @@
+"""ctypes binding of libdeco_gen.so (include/deco_gen.h): seeded synthetic systems."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+
+
+class GenParams(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("bs", C.c_int),
+        ("sigma", C.c_double), ("kz_kx", C.c_double), ("layered", C.c_int),
+        ("n_channels", C.c_int), ("channel_contrast", C.c_double), ("fault_frac", C.c_double),
+        ("n_wells", C.c_int), ("acc_lo", C.c_double), ("acc_hi", C.c_double),
+        ("cpl_lo", C.c_double), ("cpl_hi", C.c_double), ("comp", C.c_double),
+        ("smooth", C.c_int), ("seed", C.c_ulonglong),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(_PKG, "libdeco_gen.so")
+        if not os.path.exists(path):
+            from . import build
+            build.build_gen()
+        L = C.CDLL(path)
+        L.deco_gen_preset.argtypes = [C.c_int, C.c_ulonglong, C.POINTER(GenParams)]
+        L.deco_gen_size.argtypes = [C.POINTER(GenParams), C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
+        L.deco_gen_fill.argtypes = [C.POINTER(GenParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p]
+        L.deco_gen_uniform.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_longlong, C.c_void_p]
+        L.deco_gen_uniform.restype = None
+        _lib = L
+    return _lib
+
+
+@dataclass
+class System:
+    """A CSR system A x = b (reference layout: core/CSR.hpp:4-13)."""
+    n: int
+    r: np.ndarray  # int32[n+1]
+    c: np.ndarray  # int32[nnz]
+    v: np.ndarray  # float64[nnz]
+    b: np.ndarray  # float64[n]
+    bs: int
+    params: GenParams
+    logk: np.ndarray | None = None
+
+    @property
+    def nnz(self) -> int:
+        return int(self.r[-1])
+
+
+def preset(config: int, seed: int = 1234, **overrides) -> GenParams:
+    p = GenParams()
+    if lib().deco_gen_preset(config, seed, C.byref(p)) != 0:
+        raise ValueError(f"unknown preset {config}")
+    for k, val in overrides.items():
+        setattr(p, k, val)
+    return p
+
+
+def generate(p: GenParams, with_logk: bool = False) -> System:
+    n = C.c_int()
+    nnz = C.c_longlong()
+    rc = lib().deco_gen_size(C.byref(p), C.byref(n), C.byref(nnz))
+    if rc != 0:
+        raise ValueError(f"deco_gen_size failed ({rc})")
+    r = np.empty(n.value + 1, np.int32)
+    c = np.empty(nnz.value, np.int32)
+    v = np.empty(nnz.value, np.float64)
+    b = np.empty(n.value, np.float64)
+    nc = p.nx * p.ny * p.nz
+    logk = np.empty(nc, np.float64) if with_logk else None
+    rc = lib().deco_gen_fill(C.byref(p), r.ctypes.data, c.ctypes.data, v.ctypes.data, b.ctypes.data,
+                             logk.ctypes.data if logk is not None else None)
+    if rc != 0:
+        raise ValueError(f"deco_gen_fill failed ({rc})")
+    return System(n.value, r, c, v, b, p.bs, p, logk)
+
+
+def uniform(seed: int, stream: int, n: int) -> np.ndarray:
+    out = np.empty(n, np.float64)
+    lib().deco_gen_uniform(seed, stream, n, out.ctypes.data)
+    return out
+
+
+def grid(nx: int, ny: int, nz: int, bs: int = 2, seed: int = 1234, **kw) -> System:
+    """Small custom grid with the config-1 value distributions (for tests)."""
+    p = preset(1, seed)
+    p.nx, p.ny, p.nz, p.bs = nx, ny, nz, bs
+    for k, val in kw.items():
+        setattr(p, k, val)
+    return generate(p)
