@@ -92,10 +92,12 @@ def build_driver(verbose=False) -> str:
     src = os.path.join(HOST, "cpr_gpu.cpp")
     if not os.path.exists(src):
         return ""
-    deps = [src] + sorted(glob.glob(os.path.join(HOST, "*.hpp"))) + _headers() + [GPU_LIB]
+    deps = [src] + sorted(glob.glob(os.path.join(HOST, "*.hpp"))) + _headers() + [GPU_LIB, GEN_LIB]
     if _newer(DRIVER, deps):
-        _run([CXX, "-O2", "-std=c++17", "-I", INC, "-I", HOST, src, "-o", DRIVER,
-              "-L", PKG, "-ldeco_b200", "-Wl,-rpath,$ORIGIN"], verbose)
+        cuda = os.path.dirname(os.path.dirname(NVCC))
+        _run([CXX, "-O2", "-std=c++17", "-I", INC, "-I", HOST, "-I", os.path.join(cuda, "include"), src, "-o", DRIVER,
+              "-L", PKG, "-ldeco_b200", "-ldeco_gen", "-L", os.path.join(cuda, "lib64"), "-lcudart",
+              "-Wl,-rpath,$ORIGIN"], verbose)
     return DRIVER
 
 

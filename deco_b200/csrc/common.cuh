@@ -1,0 +1,165 @@
+// common.cuh — shared infrastructure of libdeco_b200: error handling across the
+// C ABI, padded device buffers, the context (device + stream + scratch), and
+// warp/block reduction helpers.  Every entry point of the C ABI returns an int
+// status (0 = ok) and never exits; deco_last_error() describes the failure.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "deco_b200.h"
+
+namespace deco {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void set_last_error(const std::string& msg);
+
+#define DECO_CUDA(call)                                                                           \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess)                                                                        \
+      throw ::deco::Error(DECO_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_) +     \
+                                             " (" + __FILE__ + ":" + std::to_string(__LINE__) + ")"); \
+  } while (0)
+
+// every kernel launch site is followed by DECO_CHECK_LAUNCH(), which also counts
+// the launch (deco_launch_count)
+void count_launch();
+#define DECO_CHECK_LAUNCH()                 \
+  do {                                      \
+    ::deco::count_launch();                 \
+    DECO_CUDA(cudaGetLastError());          \
+  } while (0)
+
+#define DECO_REQUIRE(cond, code, msg)                          \
+  do {                                                         \
+    if (!(cond)) throw ::deco::Error((code), std::string(msg)); \
+  } while (0)
+
+// Wraps a C-ABI body: converts exceptions into status codes.
+template <typename F>
+int guard(F&& f) {
+  try {
+    f();
+    return DECO_OK;
+  } catch (const Error& e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    set_last_error("host allocation failed");
+    return DECO_ERR_ALLOC;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return DECO_ERR_INTERNAL;
+  }
+}
+
+// Elements of slack after every device array: vectorised loads (16 bytes) may
+// touch up to 3 elements past the last valid one; the slack is zero-filled.
+constexpr size_t kPad = 16;
+
+// Owning device buffer with zeroed padding; moves, does not copy.
+template <typename T>
+class DevBuf {
+ public:
+  DevBuf() = default;
+  explicit DevBuf(size_t n, cudaStream_t s = 0) { alloc(n, s); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr; o.n_ = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) { release(); p_ = o.p_; n_ = o.n_; o.p_ = nullptr; o.n_ = 0; }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+
+  void alloc(size_t n, cudaStream_t s = 0) {
+    release();
+    n_ = n;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, (n + kPad) * sizeof(T));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      throw Error(DECO_ERR_ALLOC, "cudaMalloc of " + std::to_string((n + kPad) * sizeof(T)) +
+                                      " bytes failed: " + cudaGetErrorString(e));
+    }
+    p_ = static_cast<T*>(p);
+    DECO_CUDA(cudaMemsetAsync(p_ + n, 0, kPad * sizeof(T), s));
+  }
+  void zero(cudaStream_t s) {
+    if (p_) DECO_CUDA(cudaMemsetAsync(p_, 0, (n_ + kPad) * sizeof(T), s));
+  }
+  void release() {
+    if (p_) cudaFree(p_);
+    p_ = nullptr;
+    n_ = 0;
+  }
+  T* get() const { return p_; }
+  size_t size() const { return n_; }
+  explicit operator bool() const { return p_ != nullptr; }
+
+ private:
+  T* p_ = nullptr;
+  size_t n_ = 0;
+};
+
+}  // namespace deco
+
+// ----------------------------------------------------------------- handles
+
+struct deco_ctx_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int num_sms = 148;
+  int autotune = 1;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // small pinned host buffer for scalar read-backs
+  double* host_scalars = nullptr;
+  // reusable device scratch for reductions (partials + counters)
+  deco::DevBuf<double> red;
+  deco::DevBuf<unsigned int> counter;
+};
+
+namespace deco {
+
+// ------------------------------------------------------------ device helpers
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v, unsigned mask = 0xffffffffu) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+  return v;
+}
+
+template <int W, typename T>
+__device__ __forceinline__ T subwarp_sum(T v) {
+#pragma unroll
+  for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__host__ __device__ __forceinline__ long long cdiv(long long a, long long b) { return (a + b - 1) / b; }
+
+// exclusive scan of int counts[0..n) into out[0..n] (out[n] = total);
+// returns the total.  64-bit accumulation; throws if the total exceeds int32.
+long long exclusive_scan_int(deco_ctx_s* ctx, const int* counts, int* out, long long n);
+
+// grid size for a grid-stride kernel: a multiple of the SM count
+inline int grid_for(const deco_ctx_s* ctx, long long work, int block, int per_sm = 8) {
+  long long g = cdiv(work, block);
+  long long cap = (long long)ctx->num_sms * per_sm;
+  if (g > cap) g = cap;
+  return int(g < 1 ? 1 : g);
+}
+
+}  // namespace deco

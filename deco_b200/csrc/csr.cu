@@ -1,0 +1,197 @@
+// csr.cu — device CSR matrices (deco_csr), the SpMV autotuner and the SpMV /
+// residual entry points of the C ABI.
+#include <algorithm>
+
+#include "spmv.cuh"
+
+namespace deco {
+
+namespace {
+
+__global__ void row_stats(const int* __restrict__ r, int n, int* __restrict__ maxlen) {
+  int m = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    m = max(m, r[i + 1] - r[i]);
+  m = __reduce_max_sync(0xffffffffu, m);
+  if ((threadIdx.x & 31) == 0) atomicMax(maxlen, m);
+}
+
+__global__ void to_f32(const double* __restrict__ a, float* __restrict__ b, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+}  // namespace
+
+void refresh_stats(deco_ctx_s* ctx, deco_csr_s* A) {
+  DevBuf<int> mx(1, ctx->stream);
+  mx.zero(ctx->stream);
+  row_stats<<<grid_for(ctx, A->n, 256), 256, 0, ctx->stream>>>(A->r.get(), A->n, mx.get());
+  DECO_CHECK_LAUNCH();
+  DECO_CUDA(cudaMemcpyAsync(&A->max_row, mx.get(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  DECO_CUDA(cudaStreamSynchronize(ctx->stream));
+  A->avg_row = A->n ? double(A->nz) / A->n : 0.0;
+  A->sw64 = A->sw32 = 0;
+}
+
+void make_f32_values(deco_ctx_s* ctx, deco_csr_s* A) {
+  if (!A->v32 || A->v32.size() != (size_t)A->nz) A->v32.alloc(A->nz, ctx->stream);
+  to_f32<<<grid_for(ctx, A->nz, 256), 256, 0, ctx->stream>>>(A->v.get(), A->v32.get(), A->nz);
+  DECO_CHECK_LAUNCH();
+}
+
+int tuned_subwarp(deco_ctx_s* ctx, deco_csr_s* A, bool f32) {
+  int& sw = f32 ? A->sw32 : A->sw64;
+  if (sw) return sw;
+  const int W = f32 ? 4 : 2;
+  sw = heuristic_subwarp(A->avg_row, W);
+  if (!ctx->autotune || A->n < 4096) return sw;
+  cudaStreamCaptureStatus cs;
+  DECO_CUDA(cudaStreamIsCapturing(ctx->stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return sw;
+  // time each candidate on a y = A x with x = ones (values only matter for timing)
+  DevBuf<double> x(A->m, ctx->stream), y(A->n, ctx->stream);
+  DevBuf<float> xf, yf;
+  x.zero(ctx->stream);
+  if (f32) { xf.alloc(A->m, ctx->stream); yf.alloc(A->n, ctx->stream); xf.zero(ctx->stream); }
+  float best = 1e30f;
+  int best_sw = sw;
+  const int cands[] = {2, 4, 8, 16, 32};
+  for (int cand : cands) {
+    if (cand * W > 4 * (A->max_row + W) && cand > 2) continue;
+    float tot = 0.f;
+    for (int rep = 0; rep < 4; ++rep) {
+      DECO_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+      if (f32)
+        launch_spmv_sw<float, float>(ctx->stream, cand, A->n, 1, A->r.get(), A->c.get(), A->v32.get(), xf.get(),
+                                     EpiStore<float>{yf.get()});
+      else
+        launch_spmv_sw<double, double>(ctx->stream, cand, A->n, 1, A->r.get(), A->c.get(), A->v.get(), x.get(),
+                                       EpiStore<double>{y.get()});
+      DECO_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+      DECO_CUDA(cudaEventSynchronize(ctx->ev1));
+      float ms = 0.f;
+      DECO_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+      if (rep > 0) tot += ms;  // first run warms caches
+    }
+    if (tot < best) { best = tot; best_sw = cand; }
+  }
+  sw = best_sw;
+  return sw;
+}
+
+}  // namespace deco
+
+using namespace deco;
+
+extern "C" {
+
+int deco_csr_create(deco_ctx ctx, int n, int m, int nz, const int* r, const int* c, const double* v, int where,
+                    deco_csr* out) {
+  return guard([&] {
+    DECO_REQUIRE(ctx && out && r && (nz == 0 || (c && v)), DECO_ERR_ARG, "NULL argument");
+    DECO_REQUIRE(n >= 0 && m >= 0 && nz >= 0, DECO_ERR_ARG, "negative size");
+    auto* A = new deco_csr_s();
+    try {
+      A->n = n; A->m = m; A->nz = nz;
+      A->r.alloc(n + 1, ctx->stream);
+      A->c.alloc(nz, ctx->stream);
+      A->v.alloc(nz, ctx->stream);
+      cudaMemcpyKind k = where ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+      DECO_CUDA(cudaMemcpyAsync(A->r.get(), r, sizeof(int) * (n + 1), k, ctx->stream));
+      if (nz) {
+        DECO_CUDA(cudaMemcpyAsync(A->c.get(), c, sizeof(int) * (size_t)nz, k, ctx->stream));
+        DECO_CUDA(cudaMemcpyAsync(A->v.get(), v, sizeof(double) * (size_t)nz, k, ctx->stream));
+      }
+      refresh_stats(ctx, A);
+    } catch (...) {
+      delete A;
+      throw;
+    }
+    *out = A;
+  });
+}
+
+int deco_csr_destroy(deco_csr A) {
+  return guard([&] { delete A; });
+}
+
+int deco_csr_info(deco_csr A, int* n, int* m, int* nz) {
+  return guard([&] {
+    DECO_REQUIRE(A, DECO_ERR_ARG, "A is NULL");
+    if (n) *n = A->n;
+    if (m) *m = A->m;
+    if (nz) *nz = A->nz;
+  });
+}
+
+int deco_csr_download(deco_ctx ctx, deco_csr A, int* r, int* c, double* v) {
+  return guard([&] {
+    DECO_REQUIRE(ctx && A, DECO_ERR_ARG, "NULL argument");
+    if (r) DECO_CUDA(cudaMemcpyAsync(r, A->r.get(), sizeof(int) * (A->n + 1), cudaMemcpyDeviceToHost, ctx->stream));
+    if (c && A->nz) DECO_CUDA(cudaMemcpyAsync(c, A->c.get(), sizeof(int) * (size_t)A->nz, cudaMemcpyDeviceToHost, ctx->stream));
+    if (v && A->nz) DECO_CUDA(cudaMemcpyAsync(v, A->v.get(), sizeof(double) * (size_t)A->nz, cudaMemcpyDeviceToHost, ctx->stream));
+    DECO_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int deco_csr_set_values(deco_ctx ctx, deco_csr A, const double* v, int where) {
+  return guard([&] {
+    DECO_REQUIRE(ctx && A && v, DECO_ERR_ARG, "NULL argument");
+    DECO_CUDA(cudaMemcpyAsync(A->v.get(), v, sizeof(double) * (size_t)A->nz,
+                              where ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+    if (A->v32) make_f32_values(ctx, A);
+  });
+}
+
+int deco_csr_make_f32(deco_ctx ctx, deco_csr A) {
+  return guard([&] {
+    DECO_REQUIRE(ctx && A, DECO_ERR_ARG, "NULL argument");
+    make_f32_values(ctx, A);
+  });
+}
+
+int deco_csr_subwarp(deco_csr A, int* sw) {
+  return guard([&] {
+    DECO_REQUIRE(A && sw, DECO_ERR_ARG, "NULL argument");
+    *sw = A->sw64;
+  });
+}
+
+int deco_csr_set_subwarp(deco_csr A, int sw) {
+  return guard([&] {
+    DECO_REQUIRE(A, DECO_ERR_ARG, "A is NULL");
+    DECO_REQUIRE(sw == 1 || sw == 2 || sw == 4 || sw == 8 || sw == 16 || sw == 32, DECO_ERR_ARG,
+                 "sub-warp width must be a power of two in [1, 32]");
+    A->sw64 = sw;
+    A->sw32 = sw;
+  });
+}
+
+int deco_spmv(deco_ctx ctx, deco_csr A, const double* x, double* y, int bs) {
+  return guard([&] {
+    DECO_REQUIRE(ctx && A && x && y, DECO_ERR_ARG, "NULL argument");
+    DECO_REQUIRE(bs >= 1, DECO_ERR_ARG, "bs must be >= 1");
+    DECO_REQUIRE(x != y, DECO_ERR_ARG, "x and y must not alias");
+    spmv<double, double>(ctx, A, x, EpiStore<double>{y}, bs);
+  });
+}
+
+int deco_spmv_f32(deco_ctx ctx, deco_csr A, const float* x, float* y, int bs) {
+  return guard([&] {
+    DECO_REQUIRE(ctx && A && x && y, DECO_ERR_ARG, "NULL argument");
+    DECO_REQUIRE(A->v32, DECO_ERR_ARG, "matrix has no float32 values (deco_csr_make_f32)");
+    DECO_REQUIRE(bs >= 1 && x != y, DECO_ERR_ARG, "bad bs or aliasing");
+    spmv<float, float>(ctx, A, x, EpiStore<float>{y}, bs);
+  });
+}
+
+int deco_residual(deco_ctx ctx, deco_csr A, const double* b, const double* x, double* r) {
+  return guard([&] {
+    DECO_REQUIRE(ctx && A && b && x && r, DECO_ERR_ARG, "NULL argument");
+    DECO_REQUIRE(x != r, DECO_ERR_ARG, "x and r must not alias");
+    spmv<double, double>(ctx, A, x, EpiResid<double, double>{b, r});
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,647 @@
+// fsai.cu — FSAI preconditioner on the device: filters, lower pattern, batched
+// per-row dense LU grouped by order, D-scaling, transpose, apply.
+//
+// Per row i the reference (precond/FSAI/numeric.tpp:59-133, gather.cpp:14-88,
+// LU_main.cpp:14-48) gathers M = A[P,P]^T for the row's pattern P (the row of
+// lower(A) minus its last entry d), factors M with partial pivoting (dgetrf)
+// and solves  M^T fU = -A[P,d]  and  M fL = -A[d,P]^T  (dgetrs 'T' / 'N').
+// Here the same steps run with the dense arithmetic written as separately
+// rounded multiplies and adds (no FMA contraction), in the operation order of a
+// textbook LU with partial pivoting, so the factor values match the CPU
+// restatement bit for bit and the reference's LAPACK to rounding.
+//
+// Rows are grouped by order k into classes and processed in ONE launch:
+//   class 1 (1 <= k <= 8):  one thread per row, M held in registers;
+//   class 2 (8 < k <= 32):  one warp per row, M in shared memory;
+//   class 3 (32 < k <= 64): one warp per row, M in shared memory (32 KB).
+#include <algorithm>
+
+#include "fsai.cuh"
+
+namespace deco {
+
+namespace {
+
+constexpr int kLuBlock = 128;
+constexpr int kRegK = 8;
+// per warp of class 2: 32x32 system + two rhs + pivots = 8832 B, four warps per block;
+// class 3: 64x64 system + rhs + pivots = 34048 B for the block's first warp
+constexpr int kSmemBytes = 36 * 1024;
+
+__device__ __forceinline__ int bsearch_le(const int* __restrict__ a, int lo, int hi, int target) {
+  int mn = lo, mx = hi, mid = (lo + hi) >> 1;
+  while (mx - mn > 1) {
+    if (__ldg(a + mid) > target) mx = mid; else mn = mid;
+    mid = (mn + mx) >> 1;
+  }
+  return mid;
+}
+
+// a - b*c and a + b*c with two roundings (the CPU oracle is built without contraction)
+__device__ __forceinline__ double msub(double a, double b, double c) { return __dsub_rn(a, __dmul_rn(b, c)); }
+__device__ __forceinline__ double madd(double a, double b, double c) { return __dadd_rn(a, __dmul_rn(b, c)); }
+
+// ------------------------------------------------------------------ filters
+__device__ __forceinline__ bool keep_entry(int i, int col, double v, double D, double tol_rel, double tol_abs) {
+  if (col == i) return true;
+  const double a = fabs(v);
+  return (tol_rel == 0.0 || a > D) && (tol_abs == 0.0 || a > tol_abs);
+}
+
+__global__ void filter_count(int n, const int* __restrict__ r, const int* __restrict__ c,
+                             const double* __restrict__ v, double tol_rel, double tol_abs, int* __restrict__ cnt) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int a = r[i], e = r[i + 1];
+    double D = 0.0;
+    if (tol_rel != 0.0) D = fabs(__dmul_rn(v[bsearch_le(c, a, e, i)], tol_rel));
+    int k = 0;
+    for (int j = a; j < e; ++j) k += keep_entry(i, c[j], v[j], D, tol_rel, tol_abs);
+    cnt[i] = k;
+  }
+}
+
+__global__ void filter_copy(int n, const int* __restrict__ r, const int* __restrict__ c, const double* __restrict__ v,
+                            double tol_rel, double tol_abs, const int* __restrict__ ro, int* __restrict__ co,
+                            double* __restrict__ vo) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int a = r[i], e = r[i + 1];
+    double D = 0.0;
+    if (tol_rel != 0.0) D = fabs(__dmul_rn(v[bsearch_le(c, a, e, i)], tol_rel));
+    int o = ro[i];
+    for (int j = a; j < e; ++j)
+      if (keep_entry(i, c[j], v[j], D, tol_rel, tol_abs)) { co[o] = c[j]; vo[o] = v[j]; ++o; }
+  }
+}
+
+// ---------------------------------------------------------- lower(A) pattern
+// precond/FSAI/symbolic.tpp:104-148: the leading run of columns <= i
+__global__ void lower_count(int n, const int* __restrict__ r, const int* __restrict__ c, int* __restrict__ cnt) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int k = 0;
+    for (int j = r[i]; j < r[i + 1] && c[j] <= i; ++j) ++k;
+    cnt[i] = k;
+  }
+}
+
+__global__ void lower_copy(int n, const int* __restrict__ r, const int* __restrict__ c, const int* __restrict__ fr,
+                           int* __restrict__ fc) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int o = fr[i];
+    for (int j = r[i]; j < r[i + 1] && c[j] <= i; ++j) fc[o++] = c[j];
+  }
+}
+
+// ------------------------------------------------------------- row classes
+__device__ __forceinline__ int order_class(int k) { return k <= 0 ? 0 : (k <= kRegK ? 1 : (k <= 32 ? 2 : (k <= 64 ? 3 : 4))); }
+
+__global__ void class_hist(int n, const int* __restrict__ fr, int* __restrict__ hist, int* __restrict__ kmax) {
+  __shared__ int h[5];
+  if (threadIdx.x < 5) h[threadIdx.x] = 0;
+  __syncthreads();
+  int m = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int k = fr[i + 1] - fr[i] - 1;
+    atomicAdd(&h[order_class(k)], 1);
+    m = max(m, k);
+  }
+  m = __reduce_max_sync(0xffffffffu, m);
+  if ((threadIdx.x & 31) == 0) atomicMax(kmax, m);
+  __syncthreads();
+  if (threadIdx.x < 5 && h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
+}
+
+__global__ void class_scatter(int n, const int* __restrict__ fr, int* __restrict__ cursor, int* __restrict__ perm) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int cl = order_class(fr[i + 1] - fr[i] - 1);
+    if (cl >= 1 && cl <= 3) perm[atomicAdd(&cursor[cl], 1)] = i;
+  }
+}
+
+// ------------------------------------------------- class 1: thread per row
+// M(i,j) of the column-major k x k system lives in m[i][j]; every index is a
+// compile-time constant after unrolling, rows/columns >= k are predicated off.
+template <int K>
+__device__ void solve_row_reg(int i, const int* __restrict__ Ar, const int* __restrict__ Ac,
+                              const double* __restrict__ Av, const int* __restrict__ Fr, const int* __restrict__ Fc,
+                              double* __restrict__ FLv, double* __restrict__ FUv) {
+  const int a = Fr[i], e = Fr[i + 1] - 1, k = e - a;
+  const int d = Fc[e];
+  int P[K];
+#pragma unroll
+  for (int t = 0; t < K; ++t) P[t] = t < k ? Fc[a + t] : 0x7fffffff;
+  double m[K][K], rl[K], ru[K];
+#pragma unroll
+  for (int x = 0; x < K; ++x) {
+    rl[x] = 0.0; ru[x] = 0.0;
+#pragma unroll
+    for (int y = 0; y < K; ++y) m[x][y] = 0.0;
+  }
+  // gather: M(col,row) = A(P[row], P[col]);  ru[row] = -A(P[row], d)
+#pragma unroll
+  for (int row = 0; row < K; ++row) {
+    if (row < k) {
+      const int g = P[row];
+      const int ga = Ar[g], gb = Ar[g + 1];
+      int q = 0;  // merge pointer into P
+      for (int s = ga; s < gb; ++s) {
+        const int col = Ac[s];
+        while (q < k && __ldg(Fc + a + q) < col) ++q;  // pattern sorted ascending
+        if (q < k && __ldg(Fc + a + q) == col) {
+          const double val = Av[s];
+#pragma unroll
+          for (int t = 0; t < K; ++t)
+            if (t == q) m[t][row] = val;
+        }
+      }
+      const int j = bsearch_le(Ac, ga, gb, d);
+      if (Ac[j] == d) ru[row] = -Av[j];
+    }
+  }
+  {  // rl[col] = -A(d, P[col])
+    const int da = Ar[d], db = Ar[d + 1];
+    int q = 0;
+    for (int s = da; s < db; ++s) {
+      const int col = Ac[s];
+      while (q < k && __ldg(Fc + a + q) < col) ++q;
+      if (q < k && __ldg(Fc + a + q) == col) {
+        const double val = -Av[s];
+#pragma unroll
+        for (int t = 0; t < K; ++t)
+          if (t == q) rl[t] = val;
+      }
+    }
+  }
+  // LU with partial pivoting (first index of the largest |entry|)
+  int piv[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    piv[j] = j;
+    if (j < k) {
+      int p = j;
+      double best = fabs(m[j][j]);
+#pragma unroll
+      for (int x = j + 1; x < K; ++x)
+        if (x < k && fabs(m[x][j]) > best) { best = fabs(m[x][j]); p = x; }
+      piv[j] = p;
+#pragma unroll
+      for (int x = j + 1; x < K; ++x)
+        if (x == p) {
+#pragma unroll
+          for (int t = 0; t < K; ++t) { double s = m[j][t]; m[j][t] = m[x][t]; m[x][t] = s; }
+        }
+      const double dg = m[j][j];
+      if (dg != 0.0) {
+        const double inv = __ddiv_rn(1.0, dg);
+#pragma unroll
+        for (int x = j + 1; x < K; ++x)
+          if (x < k) m[x][j] = __dmul_rn(m[x][j], inv);
+      }
+#pragma unroll
+      for (int t = j + 1; t < K; ++t)
+        if (t < k) {
+          const double u = m[j][t];
+#pragma unroll
+          for (int x = j + 1; x < K; ++x)
+            if (x < k) m[x][t] = msub(m[x][t], m[x][j], u);
+        }
+    }
+  }
+  // M^T fU = ru : U^T, unit L^T, then P^T
+#pragma unroll
+  for (int j = 0; j < K; ++j)
+    if (j < k) {
+      double s = ru[j];
+#pragma unroll
+      for (int x = 0; x < j; ++x) s = msub(s, m[x][j], ru[x]);
+      ru[j] = __ddiv_rn(s, m[j][j]);
+    }
+#pragma unroll
+  for (int j = K - 1; j >= 0; --j)
+    if (j < k) {
+      double s = ru[j];
+#pragma unroll
+      for (int x = j + 1; x < K; ++x)
+        if (x < k) s = msub(s, m[x][j], ru[x]);
+      ru[j] = s;
+    }
+#pragma unroll
+  for (int j = K - 1; j >= 0; --j)
+    if (j < k && piv[j] != j) {
+#pragma unroll
+      for (int x = j + 1; x < K; ++x)
+        if (x == piv[j]) { double s = ru[j]; ru[j] = ru[x]; ru[x] = s; }
+    }
+  // M fL = rl : P, unit L, U
+#pragma unroll
+  for (int j = 0; j < K; ++j)
+    if (j < k && piv[j] != j) {
+#pragma unroll
+      for (int x = j + 1; x < K; ++x)
+        if (x == piv[j]) { double s = rl[j]; rl[j] = rl[x]; rl[x] = s; }
+    }
+#pragma unroll
+  for (int j = 0; j < K; ++j)
+    if (j < k) {
+#pragma unroll
+      for (int x = j + 1; x < K; ++x)
+        if (x < k) rl[x] = msub(rl[x], m[x][j], rl[j]);
+    }
+#pragma unroll
+  for (int j = K - 1; j >= 0; --j)
+    if (j < k) {
+      rl[j] = __ddiv_rn(rl[j], m[j][j]);
+#pragma unroll
+      for (int x = 0; x < j; ++x) rl[x] = msub(rl[x], m[x][j], rl[j]);
+    }
+#pragma unroll
+  for (int t = 0; t < K; ++t)
+    if (t < k) { FLv[a + t] = rl[t]; FUv[a + t] = ru[t]; }
+}
+
+// ------------------------------------------------- classes 2-3: warp per row
+// M column-major in shared memory: M(i,j) = sm[i + j*k].
+__device__ int find_in_pattern(const int* __restrict__ P, int k, int key) {
+  int lo = 0, hi = k - 1;
+  while (lo <= hi) {
+    int mid = (lo + hi) >> 1;
+    int v = P[mid];
+    if (v == key) return mid;
+    if (v < key) lo = mid + 1; else hi = mid - 1;
+  }
+  return -1;
+}
+
+__device__ void solve_row_warp(int i, double* __restrict__ sm, double* __restrict__ rl, double* __restrict__ ru,
+                               int* __restrict__ piv, const int* __restrict__ Ar, const int* __restrict__ Ac,
+                               const double* __restrict__ Av, const int* __restrict__ Fr,
+                               const int* __restrict__ Fc, double* __restrict__ FLv, double* __restrict__ FUv) {
+  const int lane = threadIdx.x & 31;
+  const int a = Fr[i], e = Fr[i + 1] - 1, k = e - a;
+  const int d = Fc[e];
+  const int* P = Fc + a;
+  for (int t = lane; t < k * k; t += 32) sm[t] = 0.0;
+  for (int t = lane; t < k; t += 32) { rl[t] = 0.0; ru[t] = 0.0; }
+  __syncwarp();
+  for (int row = 0; row < k; ++row) {
+    const int g = P[row];
+    const int ga = Ar[g], gb = Ar[g + 1];
+    for (int s = ga + lane; s < gb; s += 32) {
+      const int col = Ac[s];
+      const int q = find_in_pattern(P, k, col);
+      if (q >= 0) sm[q + row * k] = Av[s];
+      if (col == d) ru[row] = -Av[s];
+    }
+  }
+  {
+    const int da = Ar[d], db = Ar[d + 1];
+    for (int s = da + lane; s < db; s += 32) {
+      const int q = find_in_pattern(P, k, Ac[s]);
+      if (q >= 0) rl[q] = -Av[s];
+    }
+  }
+  __syncwarp();
+  // LU with partial pivoting
+  for (int j = 0; j < k; ++j) {
+    double best = -1.0;
+    int p = 0x7fffffff;
+    for (int x = j + lane; x < k; x += 32) {
+      double v = fabs(sm[x + j * k]);
+      if (v > best) { best = v; p = x; }  // rows visited in increasing order per lane
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      int op = __shfl_xor_sync(0xffffffffu, p, o);
+      if (ob > best || (ob == best && op < p)) { best = ob; p = op; }
+    }
+    // first index of the maximum, as a sequential scan with strict '>' finds
+    if (lane == 0) piv[j] = p;
+    if (p != j)
+      for (int t = lane; t < k; t += 32) {
+        double s = sm[j + t * k];
+        sm[j + t * k] = sm[p + t * k];
+        sm[p + t * k] = s;
+      }
+    __syncwarp();
+    const double dg = sm[j + j * k];
+    if (dg != 0.0) {
+      const double inv = __ddiv_rn(1.0, dg);
+      for (int x = j + 1 + lane; x < k; x += 32) sm[x + j * k] = __dmul_rn(sm[x + j * k], inv);
+    }
+    __syncwarp();
+    for (int t = j + 1; t < k; ++t) {
+      const double u = sm[j + t * k];
+      for (int x = j + 1 + lane; x < k; x += 32) sm[x + t * k] = msub(sm[x + t * k], sm[x + j * k], u);
+    }
+    __syncwarp();
+  }
+  // M^T fU = ru (lane 0 runs the short recurrences; k <= 64)
+  if (lane == 0) {
+    for (int j = 0; j < k; ++j) {
+      double s = ru[j];
+      for (int x = 0; x < j; ++x) s = msub(s, sm[x + j * k], ru[x]);
+      ru[j] = __ddiv_rn(s, sm[j + j * k]);
+    }
+    for (int j = k - 1; j >= 0; --j) {
+      double s = ru[j];
+      for (int x = j + 1; x < k; ++x) s = msub(s, sm[x + j * k], ru[x]);
+      ru[j] = s;
+    }
+    for (int j = k - 1; j >= 0; --j)
+      if (piv[j] != j) { double s = ru[j]; ru[j] = ru[piv[j]]; ru[piv[j]] = s; }
+    for (int j = 0; j < k; ++j)
+      if (piv[j] != j) { double s = rl[j]; rl[j] = rl[piv[j]]; rl[piv[j]] = s; }
+  }
+  __syncwarp();
+  // M fL = rl: forward with unit L, backward with U (lanes over rows)
+  for (int j = 0; j < k; ++j) {
+    const double bj = rl[j];
+    for (int x = j + 1 + lane; x < k; x += 32) rl[x] = msub(rl[x], sm[x + j * k], bj);
+    __syncwarp();
+  }
+  for (int j = k - 1; j >= 0; --j) {
+    if (lane == 0) rl[j] = __ddiv_rn(rl[j], sm[j + j * k]);
+    __syncwarp();
+    const double bj = rl[j];
+    for (int x = lane; x < j; x += 32) rl[x] = msub(rl[x], sm[x + j * k], bj);
+    __syncwarp();
+  }
+  for (int t = lane; t < k; t += 32) { FLv[a + t] = rl[t]; FUv[a + t] = ru[t]; }
+  __syncwarp();
+}
+
+// one launch: blocks [0,b1) class 1, [b1,b1+b2) class 2, then class 3
+__global__ void __launch_bounds__(kLuBlock) fsai_local_systems(
+    const int* __restrict__ perm, int n1, int n2, int n3, int b1, int b2, const int* __restrict__ Ar,
+    const int* __restrict__ Ac, const double* __restrict__ Av, const int* __restrict__ Fr,
+    const int* __restrict__ Fc, double* __restrict__ FLv, double* __restrict__ FUv) {
+  extern __shared__ double smem[];
+  const int b = blockIdx.x;
+  if (b < b1) {
+    const int q = b * kLuBlock + threadIdx.x;
+    if (q < n1) solve_row_reg<kRegK>(perm[q], Ar, Ac, Av, Fr, Fc, FLv, FUv);
+    return;
+  }
+  const int warp = threadIdx.x >> 5;
+  if (b < b1 + b2) {
+    const int q = (b - b1) * (kLuBlock / 32) + warp;
+    if (q >= n2) return;
+    // per warp: 32x32 system + rhs + pivots
+    double* base = smem + warp * (32 * 32 + 64 + 16);
+    solve_row_warp(perm[n1 + q], base, base + 32 * 32, base + 32 * 32 + 32, reinterpret_cast<int*>(base + 32 * 32 + 64),
+                   Ar, Ac, Av, Fr, Fc, FLv, FUv);
+    return;
+  }
+  const int q = b - b1 - b2;
+  if (warp != 0 || q >= n3) return;
+  double* base = smem;  // 64x64 system (32 KB), then rhs and pivots
+  double* rl = smem + 64 * 64;
+  solve_row_warp(perm[n1 + n2 + q], base, rl, rl + 64, reinterpret_cast<int*>(rl + 128), Ar, Ac, Av, Fr, Fc, FLv,
+                 FUv);
+}
+
+// ------------------------------------------------- D-scaling (diagonal.cpp)
+// Row i only reads its own FL/FU rows and rows of A, so the diagonal reset, D_i
+// and the scaling of row i fuse into one thread.
+__global__ void fsai_scale(int n, const int* __restrict__ Ar, const int* __restrict__ Ac,
+                           const double* __restrict__ Av, const int* __restrict__ Fr, const int* __restrict__ Fc,
+                           double* __restrict__ FLv, double* __restrict__ FUv) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int aF = Fr[i], bF = Fr[i + 1];
+    if (bF == aF) continue;  // an empty pattern row has no diagonal to set
+    FLv[bF - 1] = 1.0;
+    FUv[bF - 1] = 1.0;
+    double sum = 0.0;
+    for (int j = aF; j < bF; ++j) {
+      const double fl = FLv[j];
+      if (fl != 0.0) {
+        const int colF = Fc[j];
+        int pa = Ar[colF], pb = Ar[colF + 1], pu = aF;
+        double s = 0.0;
+        while (pa < pb && pu < bF) {
+          const int ca = Ac[pa], cu = Fc[pu];
+          if (ca == cu) { s = madd(s, Av[pa], FUv[pu]); ++pa; ++pu; }
+          else if (ca < cu) ++pa;
+          else ++pu;
+        }
+        sum = madd(sum, fl, s);
+      }
+    }
+    const double D = (sum < 0.0) ? -__ddiv_rn(1.0, __dsqrt_rn(fabs(sum))) : __ddiv_rn(1.0, __dsqrt_rn(sum));
+    const double Da = fabs(D);
+    for (int j = aF; j < bF; ++j) {
+      FLv[j] = __dmul_rn(FLv[j], D);
+      FUv[j] = __dmul_rn(FUv[j], Da);
+    }
+  }
+}
+
+// ------------------------------------------------------- transpose (CSR.hpp)
+__global__ void col_count(long long nz, const int* __restrict__ c, int* __restrict__ cnt) {
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nz; j += (long long)gridDim.x * blockDim.x)
+    atomicAdd(&cnt[c[j]], 1);
+}
+
+__global__ void col_scatter(int n, const int* __restrict__ r, const int* __restrict__ c, const double* __restrict__ v,
+                            int* __restrict__ cursor, int* __restrict__ tc, double* __restrict__ tv) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    for (int j = r[i]; j < r[i + 1]; ++j) {
+      const int pos = atomicAdd(&cursor[c[j]], 1);
+      tc[pos] = i;
+      tv[pos] = v[j];
+    }
+}
+
+// rows of the transpose get their entries in ascending source-row order, the
+// order the reference's sequential scatter produces (CSR.hpp:193-206)
+__global__ void sort_rows(int n, const int* __restrict__ r, int* __restrict__ c, double* __restrict__ v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int a = r[i], e = r[i + 1];
+    for (int j = a + 1; j < e; ++j) {
+      const int key = c[j];
+      const double val = v[j];
+      int t = j - 1;
+      while (t >= a && c[t] > key) { c[t + 1] = c[t]; v[t + 1] = v[t]; --t; }
+      c[t + 1] = key;
+      v[t + 1] = val;
+    }
+  }
+}
+
+}  // namespace
+
+void csr_filter(deco_ctx_s* ctx, const deco_csr_s* A, double tol_rel, double tol_abs, deco_csr_s* out) {
+  cudaStream_t st = ctx->stream;
+  const int n = A->n;
+  DevBuf<int> cnt(n + 1, st);
+  const int g = grid_for(ctx, n, 256);
+  filter_count<<<g, 256, 0, st>>>(n, A->r.get(), A->c.get(), A->v.get(), tol_rel, tol_abs, cnt.get());
+  DECO_CHECK_LAUNCH();
+  out->n = n;
+  out->m = A->m;
+  out->r.alloc(n + 1, st);
+  out->nz = (int)exclusive_scan_int(ctx, cnt.get(), out->r.get(), n);
+  out->c.alloc(out->nz, st);
+  out->v.alloc(out->nz, st);
+  filter_copy<<<g, 256, 0, st>>>(n, A->r.get(), A->c.get(), A->v.get(), tol_rel, tol_abs, out->r.get(),
+                                 out->c.get(), out->v.get());
+  DECO_CHECK_LAUNCH();
+  refresh_stats(ctx, out);
+}
+
+void csr_filter_inplace(deco_ctx_s* ctx, deco_csr_s* A, double tol_rel, double tol_abs) {
+  deco_csr_s B;
+  csr_filter(ctx, A, tol_rel, tol_abs, &B);
+  A->nz = B.nz;
+  A->r = std::move(B.r);
+  A->c = std::move(B.c);
+  A->v = std::move(B.v);
+  if (A->v32) make_f32_values(ctx, A);
+  refresh_stats(ctx, A);
+}
+
+void fsai_build(deco_ctx_s* ctx, const deco_csr_s* A0, double tol_rel, double tol_abs, int power, int precision,
+                deco_fsai_s* F) {
+  cudaStream_t st = ctx->stream;
+  DECO_REQUIRE(A0->n == A0->m, DECO_ERR_ARG, "FSAI needs a square matrix");
+  DECO_REQUIRE(power == 1, DECO_ERR_UNSUPPORTED, "FSAI power 2 (lower(A^2) pattern) is not available on the GPU path");
+  DECO_REQUIRE(precision == 64 || precision == 32, DECO_ERR_ARG, "precision must be 64 or 32");
+  const int n = A0->n;
+  F->n = n;
+  F->precision = precision;
+  // 1. filtered copy (FSAI.hpp:22-28)
+  deco_csr_s Af;
+  const deco_csr_s* A = A0;
+  if (tol_rel != 0.0 || tol_abs != 0.0) {
+    csr_filter(ctx, A0, tol_rel, tol_abs, &Af);
+    A = &Af;
+  }
+  const int g = grid_for(ctx, n, 256);
+  // 2. symbolic: lower(A)
+  DevBuf<int> cnt(n + 1, st);
+  lower_count<<<g, 256, 0, st>>>(n, A->r.get(), A->c.get(), cnt.get());
+  DECO_CHECK_LAUNCH();
+  deco_csr_s& FL = F->FL;
+  FL.n = FL.m = n;
+  FL.r.alloc(n + 1, st);
+  FL.nz = (int)exclusive_scan_int(ctx, cnt.get(), FL.r.get(), n);
+  FL.c.alloc(FL.nz, st);
+  FL.v.alloc(FL.nz, st);
+  FL.v.zero(st);
+  lower_copy<<<g, 256, 0, st>>>(n, A->r.get(), A->c.get(), FL.r.get(), FL.c.get());
+  DECO_CHECK_LAUNCH();
+  F->nz = FL.nz;
+  DevBuf<double> fu(FL.nz, st);  // FU values in FL's (lower) layout before the transpose
+  fu.zero(st);
+  // 3. group rows by order and solve the local systems in one launch
+  DevBuf<int> hist(16, st);
+  hist.zero(st);
+  class_hist<<<g, 256, 0, st>>>(n, FL.r.get(), hist.get(), hist.get() + 8);
+  DECO_CHECK_LAUNCH();
+  int h[16];
+  DECO_CUDA(cudaMemcpyAsync(h, hist.get(), sizeof(h), cudaMemcpyDeviceToHost, st));
+  DECO_CUDA(cudaStreamSynchronize(st));
+  F->max_order = h[8];
+  DECO_REQUIRE(h[4] == 0, DECO_ERR_UNSUPPORTED,
+               "FSAI local system of order " + std::to_string(h[8]) + " exceeds the supported maximum of 64");
+  const int n1 = h[1], n2 = h[2], n3 = h[3];
+  const int nsolve = n1 + n2 + n3;
+  if (nsolve > 0) {
+    DevBuf<int> perm(nsolve, st);
+    int cur[4] = {0, 0, n1, n1 + n2};
+    DevBuf<int> cursor(4, st);
+    DECO_CUDA(cudaMemcpyAsync(cursor.get(), cur, sizeof(cur), cudaMemcpyHostToDevice, st));
+    class_scatter<<<g, 256, 0, st>>>(n, FL.r.get(), cursor.get(), perm.get());
+    DECO_CHECK_LAUNCH();
+    const int b1 = (int)cdiv(n1, kLuBlock), b2 = (int)cdiv(n2, kLuBlock / 32), b3 = n3;
+    const size_t smem = (n2 + n3) > 0 ? kSmemBytes : 0;
+    if (smem) DECO_CUDA(cudaFuncSetAttribute(fsai_local_systems, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+    fsai_local_systems<<<b1 + b2 + b3, kLuBlock, smem, st>>>(perm.get(), n1, n2, n3, b1, b2, A->r.get(),
+                                                                A->c.get(), A->v.get(), FL.r.get(), FL.c.get(),
+                                                                FL.v.get(), fu.get());
+    DECO_CHECK_LAUNCH();
+  }
+  // 4. D = diag(FL A FU^T); FL *= D, FU *= |D|  (diagonal.cpp:6-73)
+  fsai_scale<<<g, 256, 0, st>>>(n, A->r.get(), A->c.get(), A->v.get(), FL.r.get(), FL.c.get(), FL.v.get(), fu.get());
+  DECO_CHECK_LAUNCH();
+  // 5. FU^T (trans_mat_full)
+  deco_csr_s& U = F->FUt;
+  U.n = U.m = n;
+  U.nz = FL.nz;
+  DevBuf<int> ccount(n + 1, st);
+  ccount.zero(st);
+  col_count<<<grid_for(ctx, FL.nz, 256), 256, 0, st>>>(FL.nz, FL.c.get(), ccount.get());
+  DECO_CHECK_LAUNCH();
+  U.r.alloc(n + 1, st);
+  exclusive_scan_int(ctx, ccount.get(), U.r.get(), n);
+  U.c.alloc(U.nz, st);
+  U.v.alloc(U.nz, st);
+  DECO_CUDA(cudaMemcpyAsync(ccount.get(), U.r.get(), sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
+  col_scatter<<<g, 256, 0, st>>>(n, FL.r.get(), FL.c.get(), fu.get(), ccount.get(), U.c.get(), U.v.get());
+  DECO_CHECK_LAUNCH();
+  sort_rows<<<g, 256, 0, st>>>(n, U.r.get(), U.c.get(), U.v.get());
+  DECO_CHECK_LAUNCH();
+  refresh_stats(ctx, &FL);
+  refresh_stats(ctx, &U);
+  F->tmp.alloc(n, st);
+  if (precision == 32) {
+    make_f32_values(ctx, &FL);
+    make_f32_values(ctx, &U);
+    F->tmp32.alloc(n, st);
+  }
+  DECO_CUDA(cudaStreamSynchronize(st));
+}
+
+}  // namespace deco
+
+using namespace deco;
+
+extern "C" {
+
+int deco_fsai_create(deco_ctx ctx, deco_csr A, double tol_rel, double tol_abs, int power, int precision,
+                     deco_fsai* out) {
+  return guard([&] {
+    DECO_REQUIRE(ctx && A && out, DECO_ERR_ARG, "NULL argument");
+    auto* F = new deco_fsai_s();
+    try {
+      fsai_build(ctx, A, tol_rel, tol_abs, power, precision, F);
+    } catch (...) {
+      delete F;
+      throw;
+    }
+    *out = F;
+  });
+}
+
+int deco_fsai_destroy(deco_fsai F) {
+  return guard([&] { delete F; });
+}
+
+int deco_fsai_info(deco_fsai F, int* n, int* nz, int* max_order) {
+  return guard([&] {
+    DECO_REQUIRE(F, DECO_ERR_ARG, "F is NULL");
+    if (n) *n = F->n;
+    if (nz) *nz = F->nz;
+    if (max_order) *max_order = F->max_order;
+  });
+}
+
+int deco_fsai_download(deco_ctx ctx, deco_fsai F, int* Lr, int* Lc, double* Lv, int* Ur, int* Uc, double* Uv) {
+  int rc = deco_csr_download(ctx, &F->FL, Lr, Lc, Lv);
+  if (rc) return rc;
+  return deco_csr_download(ctx, &F->FUt, Ur, Uc, Uv);
+}
+
+int deco_fsai_apply(deco_ctx ctx, deco_fsai F, const double* x, double* y) {
+  return guard([&] {
+    DECO_REQUIRE(ctx && F && x && y, DECO_ERR_ARG, "NULL argument");
+    if (F->precision == 32) {
+      spmv<float, double>(ctx, &F->FL, x, EpiStore<float>{F->tmp32.get()});
+      spmv<float, float>(ctx, &F->FUt, F->tmp32.get(), EpiStore<double>{y});
+    } else {
+      fsai_apply_t<double, double, double>(ctx, F, x, F->tmp.get(), EpiStore<double>{y});
+    }
+  });
+}
+
+}  // extern "C"

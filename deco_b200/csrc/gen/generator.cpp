@@ -4,9 +4,10 @@
 //   a = 0      total / pressure equation: sum_t T_st (p_s - p_t) + compressibility
 //   a = 1..bs-1 phase equations: upwinded fractional flow f_a(S_up) * T (p_s - p_t)
 //              + accumulation phi V / dt on the phase's own saturation.
-// Saturation derivatives of the face fluxes are upwinded: the upstream cell gets
-// +c on its diagonal block, the downstream cell -c on the off-diagonal block, and
-// the non-upwind side keeps a tiny entry so that every coupling block is dense.
+// Saturation derivatives of the face fluxes are upwinded along a seeded flow
+// potential: the upstream cell gets +c on its diagonal block, the downstream cell
+// -c on the off-diagonal block, and the non-upwind side keeps a tiny entry so that
+// every coupling block is dense.
 // Wells are vertical columns that add a productivity index to the pressure
 // diagonal (and f_a * PI to the phase rows), which anchors the elliptic block.
 #include "../../../include/deco_gen.h"
@@ -169,10 +170,12 @@ void build_logk(Sys& s) {
           if (std::fabs(y - yc) <= hw) in_channel[(long long)x + (long long)s.nx * (y + (long long)s.ny * z)] = 1;
       }
   }
+  // channel cells carry permeability contrast x the background median (ln k = 0):
+  // the contrast is between channel and matrix, not on top of the matrix's tail
   if (p->n_channels > 0) {
 #pragma omp parallel for
     for (long long i = 0; i < nc; ++i)
-      if (in_channel[i]) s.logk[i] += lc;
+      if (in_channel[i]) s.logk[i] = lc + 0.1 * p->sigma * gauss(p->seed, S_CHAN + 100, (uint64_t)i);
   }
 }
 
@@ -215,6 +218,15 @@ double face_mult(const Sys& s, int a, int b) {
   return 0.5;
 }
 
+// flow potential: a regional gradient (mostly +x) plus a small per-cell jitter;
+// the upstream cell of every face is the one with the higher potential, so the
+// upwinded saturation couplings never form a cycle
+inline double potential(const Sys& s, int c) {
+  const int x = c % s.nx, y = (c / s.nx) % s.ny;
+  const long long z = (long long)c / ((long long)s.nx * s.ny);
+  return -(x + 0.37 * y + 0.13 * (double)z) + 0.3 * uni(s.p->seed, S_FACE, (uint64_t)c);
+}
+
 struct CellData {
   double acc, fr[3];
 };
@@ -253,7 +265,7 @@ int deco_gen_preset(int config, unsigned long long seed, deco_gen_params* p) {
     case 2: p->nx = 100; p->ny = 100; p->nz = 50; p->bs = 3; p->sigma = 2.0; p->layered = 1;
             p->kz_kx = 0.1; p->fault_frac = 0.01; break;
     case 3: p->nx = 200; p->ny = 200; p->nz = 100; p->bs = 2; p->sigma = 2.5; p->n_channels = 6;
-            p->channel_contrast = 1e4; break;
+            p->channel_contrast = 1e4; p->comp = 1.0; break;
     case 5: p->nx = 64; p->ny = 64; p->nz = 32; p->bs = 2; p->sigma = 1.5; break;
     default: return -1;
   }
@@ -325,8 +337,8 @@ int deco_gen_fill(const deco_gen_params* p, int* r, int* c, double* v, double* b
       const uint64_t fid = (uint64_t)fa * 2654435761ull ^ ((uint64_t)fb << 20) ^ (uint64_t)fb;
       const double kt = std::exp(s.logk[t]);
       const double T = 2.0 * ks * kt / (ks + kt) * face_mult(s, fa, fb);
-      const bool up_is_a = (hsh(p->seed, S_FACE, fid) & 1) != 0;
-      const int up = up_is_a ? fa : fb;
+      // upwind side from a seeded flow potential (acyclic, as a real flux field is)
+      const int up = potential(s, fa) > potential(s, fb) ? fa : fb;
       const double g = logu(p->cpl_lo, p->cpl_hi, uni(p->seed, S_FACE_G, fid));
       const CellData ud = (up == cs) ? me : cell_data(s, up);
       double (*Ob)[3] = O[q];

@@ -1,0 +1,147 @@
+// spmv.cuh — CSR sparse matrix-vector product for sm_100a, and the device
+// CSR handle.
+//
+// Algorithm (the reference's alg::spmv, core/alg.hpp:50-64, computes the same
+// sums row by row in column order):
+//   * a sub-warp of SW lanes (1..32, chosen per matrix by the autotuner) owns a
+//     row; lanes stride over the row with 128-bit loads of values (double2 /
+//     float4) and the matching 64/128-bit loads of column indices, starting
+//     from the row start rounded down to the vector width and masking entries
+//     outside the row, so every load is aligned and coalesced across the
+//     sub-warps of a warp;
+//   * values and columns stream through with evict-first loads, x is read
+//     through the read-only path (L1/L2 keep the 7-point stencil's x tiles);
+//   * sums accumulate in float64 and are reduced with warp shuffles;
+//   * the epilogue fuses the vector operation that follows the product in the
+//     CPR and GMRES sequences (store, accumulate, residual, pressure
+//     restriction, pressure prolongation), so those never cost a pass of
+//     their own.
+#pragma once
+#include "common.cuh"
+
+struct deco_csr_s {
+  int n = 0, m = 0, nz = 0;
+  deco::DevBuf<int> r, c;
+  deco::DevBuf<double> v;
+  deco::DevBuf<float> v32;
+  int sw64 = 0, sw32 = 0;   // sub-warp width per value precision (0 = not chosen yet)
+  int max_row = 0;
+  double avg_row = 0;
+};
+
+namespace deco {
+
+template <typename VT> struct Vec;
+template <> struct Vec<double> { using V = double2; using I = int2; static constexpr int W = 2; };
+template <> struct Vec<float> { using V = float4; using I = int4; static constexpr int W = 4; };
+
+__device__ __forceinline__ double2 ld_stream(const double2* p) { return __ldcs(p); }
+__device__ __forceinline__ float4 ld_stream(const float4* p) { return __ldcs(p); }
+__device__ __forceinline__ int2 ld_stream(const int2* p) { return __ldcs(p); }
+__device__ __forceinline__ int4 ld_stream(const int4* p) { return __ldcs(p); }
+
+__device__ __forceinline__ double elem(const double2& v, int q) { return q == 0 ? v.x : v.y; }
+__device__ __forceinline__ double elem(const float4& v, int q) {
+  return q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w));
+}
+__device__ __forceinline__ int elem(const int2& v, int q) { return q == 0 ? v.x : v.y; }
+__device__ __forceinline__ int elem(const int4& v, int q) {
+  return q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w));
+}
+
+// ----------------------------------------------------------------- epilogues
+template <typename YT> struct EpiStore {
+  YT* y;
+  __device__ void operator()(int o, double s) const { y[o] = (YT)s; }
+};
+template <typename YT> struct EpiAdd {
+  YT* y;
+  __device__ void operator()(int o, double s) const { y[o] = (YT)((double)y[o] + s); }
+};
+template <typename ZT, typename YT> struct EpiResid {  // y = z - A x
+  const ZT* z; YT* y;
+  __device__ void operator()(int o, double s) const { y[o] = (YT)((double)z[o] - s); }
+};
+template <typename ZT, typename YT> struct EpiRestrict {  // y[s] = r[s*bs+p] - (A x)[s*bs]
+  const ZT* r; YT* y; int bs, p;
+  __device__ void operator()(int o, double s) const { y[o] = (YT)((double)r[(long long)o * bs + p] - s); }
+};
+template <typename YT> struct EpiProlong {  // x[s*bs+p] += (F t)[s]
+  YT* x; int bs, p;
+  __device__ void operator()(int o, double s) const {
+    long long i = (long long)o * bs + p;
+    x[i] = (YT)((double)x[i] + s);
+  }
+};
+
+// ---------------------------------------------------------------- the kernel
+template <int SW, typename VT, typename XT, class Epi>
+__global__ void __launch_bounds__(256) spmv_kernel(int nrows_out, int row_stride, const int* __restrict__ rp,
+                                                   const int* __restrict__ ci, const VT* __restrict__ vv,
+                                                   const XT* __restrict__ x, Epi epi) {
+  using VV = typename Vec<VT>::V;
+  using VI = typename Vec<VT>::I;
+  constexpr int W = Vec<VT>::W;
+  const int lane = threadIdx.x & (SW - 1);
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int orow = int(gid / SW);
+  const bool valid = orow < nrows_out;
+  double sum = 0.0;
+  if (valid) {
+    const long long row = (long long)orow * row_stride;
+    const int a = __ldg(rp + row), e = __ldg(rp + row + 1);
+    for (int k = (a & ~(W - 1)) + lane * W; k < e; k += SW * W) {
+      const VV v4 = ld_stream(reinterpret_cast<const VV*>(vv + k));
+      const VI c4 = ld_stream(reinterpret_cast<const VI*>(ci + k));
+#pragma unroll
+      for (int q = 0; q < W; ++q) {
+        const int idx = k + q;
+        if (idx >= a && idx < e) sum += elem(v4, q) * (double)__ldg(x + elem(c4, q));
+      }
+    }
+  }
+  if (SW > 1) sum = subwarp_sum<SW>(sum);
+  if (valid && lane == 0) epi(orow, sum);
+}
+
+template <typename VT, typename XT, class Epi>
+void launch_spmv_sw(cudaStream_t st, int sw, int nrows_out, int row_stride, const int* r, const int* c,
+                    const VT* v, const XT* x, Epi epi) {
+  if (nrows_out <= 0) return;
+  const int block = 256;
+  const long long threads = (long long)nrows_out * sw;
+  const unsigned grid = (unsigned)cdiv(threads, block);
+  switch (sw) {
+    case 1: spmv_kernel<1, VT, XT, Epi><<<grid, block, 0, st>>>(nrows_out, row_stride, r, c, v, x, epi); break;
+    case 2: spmv_kernel<2, VT, XT, Epi><<<grid, block, 0, st>>>(nrows_out, row_stride, r, c, v, x, epi); break;
+    case 4: spmv_kernel<4, VT, XT, Epi><<<grid, block, 0, st>>>(nrows_out, row_stride, r, c, v, x, epi); break;
+    case 8: spmv_kernel<8, VT, XT, Epi><<<grid, block, 0, st>>>(nrows_out, row_stride, r, c, v, x, epi); break;
+    case 16: spmv_kernel<16, VT, XT, Epi><<<grid, block, 0, st>>>(nrows_out, row_stride, r, c, v, x, epi); break;
+    default: spmv_kernel<32, VT, XT, Epi><<<grid, block, 0, st>>>(nrows_out, row_stride, r, c, v, x, epi); break;
+  }
+  DECO_CHECK_LAUNCH();
+}
+
+// heuristic width: enough lanes that one pass of vector loads covers the row
+inline int heuristic_subwarp(double avg_row, int W) {
+  double loads = avg_row / W + 1.0;
+  int sw = 1;
+  while (sw < 32 && sw < loads) sw <<= 1;
+  return sw;
+}
+
+// Chooses (and caches) the sub-warp width of A for float64 (f32 = false) or
+// float32 values: heuristic, refined by timing candidates when ctx->autotune.
+int tuned_subwarp(deco_ctx_s* ctx, deco_csr_s* A, bool f32);
+
+// y = op(A x) over rows 0, bs, 2bs, ... (nrows_out = n / bs rows)
+template <typename VT, typename XT, class Epi>
+void spmv(deco_ctx_s* ctx, deco_csr_s* A, const XT* x, Epi epi, int bs = 1) {
+  const bool f32 = sizeof(VT) == 4;
+  const int sw = tuned_subwarp(ctx, A, f32);
+  const VT* v;
+  if constexpr (sizeof(VT) == 4) v = A->v32.get(); else v = A->v.get();
+  launch_spmv_sw<VT, XT, Epi>(ctx->stream, sw, (A->n + bs - 1) / bs, bs, A->r.get(), A->c.get(), v, x, epi);
+}
+
+}  // namespace deco

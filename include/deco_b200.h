@@ -1,0 +1,188 @@
+/*
+ * deco_b200.h — C ABI of the B200 CPR-Krylov path (libdeco_b200.so).
+ *
+ * This is the drop-in boundary for the reference's hot path (amavliut/deco):
+ * the reference's C++ classes CSR, FSAI, CPR and SOL (header-only templates,
+ * core/CSR.hpp, precond/FSAI/FSAI.hpp, precond/CPR.hpp, solver/SOL.hpp) are
+ * re-expressed on the host side as thin C++ classes (deco_b200/host/*.hpp)
+ * that forward to the functions below.  Signatures use plain pointers and
+ * sizes only.
+ *
+ * Conventions
+ *   - Matrices are CSR<int,int,double> exactly as in the reference
+ *     (core/CSR.hpp:6-13): int32 row pointers r[n+1], int32 sorted columns
+ *     c[nz], float64 values v[nz]; cell-major unknowns, pressure id p.
+ *   - Every call returns DECO_OK (0) or a negative DECO_ERR_* code; the
+ *     message is in deco_last_error() (per host thread).  Nothing exits the
+ *     process (the reference calls exit() on zero pivots: precond/CPR.hpp:416,
+ *     643, 665; solver/rgmres.tpp:96-99 — here those are DECO_ERR_SINGULAR /
+ *     DECO_ERR_BREAKDOWN statuses).
+ *   - Vector arguments named d_* are device pointers (float64 unless stated);
+ *     h_* are host pointers.  Calls are ordered on the context's stream;
+ *     functions returning host data synchronise that stream.
+ *   - Handles are not thread-safe; one host thread per context.
+ */
+#ifndef DECO_B200_H
+#define DECO_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define DECO_OK 0
+#define DECO_ERR_ARG (-1)        /* invalid argument                         */
+#define DECO_ERR_CUDA (-2)       /* CUDA runtime error                       */
+#define DECO_ERR_ALLOC (-3)      /* device or host allocation failed         */
+#define DECO_ERR_SINGULAR (-4)   /* zero determinant / pivot in a cell block */
+#define DECO_ERR_BREAKDOWN (-5)  /* zero Hessenberg diagonal in GMRES        */
+#define DECO_ERR_UNSUPPORTED (-6)/* option not implemented on this path      */
+#define DECO_ERR_PATTERN (-7)    /* matrix layout assumption violated        */
+#define DECO_ERR_INTERNAL (-8)
+
+typedef struct deco_ctx_s* deco_ctx;
+typedef struct deco_csr_s* deco_csr;
+typedef struct deco_fsai_s* deco_fsai;
+typedef struct deco_cpr_s* deco_cpr;
+
+/* Last error message of the calling host thread ("" if none). */
+const char* deco_last_error(void);
+/* Library version string. */
+const char* deco_version(void);
+/* Kernels this library has launched in this process (all contexts). */
+long long deco_launch_count(void);
+
+/* ------------------------------------------------------------------ context
+ * Replaces the reference's process-global state (MPI_Comm deco_comm,
+ * core/pch.h:23; OpenMP thread pool).  stream == NULL creates a private
+ * non-blocking stream. */
+int deco_ctx_create(int device, void* stream, deco_ctx* out);
+int deco_ctx_destroy(deco_ctx ctx);
+int deco_ctx_sync(deco_ctx ctx);
+int deco_ctx_stream(deco_ctx ctx, void** stream);
+/* autotune != 0: SpMV sub-warp width is chosen per matrix by timing (default 1). */
+int deco_ctx_set_autotune(deco_ctx ctx, int autotune);
+
+/* --------------------------------------------------------------- matrices
+ * Replaces CSR<int,int,double> construction and its raw arrays
+ * (core/CSR.hpp:45-70) on the device.  where = 0: arrays are host memory;
+ * where = 1: arrays are device memory (copied).  The matrix keeps float64
+ * values; deco_csr_make_f32() adds a float32 copy used by mixed precision. */
+int deco_csr_create(deco_ctx ctx, int n, int m, int nz, const int* r, const int* c, const double* v,
+                    int where, deco_csr* out);
+int deco_csr_destroy(deco_csr A);
+int deco_csr_info(deco_csr A, int* n, int* m, int* nz);
+/* Copies the current (possibly CPR-modified) arrays to host buffers. */
+int deco_csr_download(deco_ctx ctx, deco_csr A, int* h_r, int* h_c, double* h_v);
+/* Overwrite values (same pattern) from host (where=0) or device (where=1). */
+int deco_csr_set_values(deco_ctx ctx, deco_csr A, const double* v, int where);
+int deco_csr_make_f32(deco_ctx ctx, deco_csr A);
+/* SpMV sub-warp width in use (1..32) and the one the autotuner picked. */
+int deco_csr_subwarp(deco_csr A, int* sw);
+int deco_csr_set_subwarp(deco_csr A, int sw);
+
+/* y = A x (bs == 1), or the restricted product of alg::spmv with bs > 1:
+ * y[i/bs] = (A x)[i] for rows i = 0, bs, 2bs, ...   (core/alg.hpp:50-64,
+ * CSR::apply core/CSR.hpp:132-136).  d_x and d_y must not alias. */
+int deco_spmv(deco_ctx ctx, deco_csr A, const double* d_x, double* d_y, int bs);
+/* float32 values + float32 vectors (requires deco_csr_make_f32). */
+int deco_spmv_f32(deco_ctx ctx, deco_csr A, const float* d_x, float* d_y, int bs);
+/* d_r = d_b - A d_x (the residual the solvers form, solver/rgmres.tpp:43-47). */
+int deco_residual(deco_ctx ctx, deco_csr A, const double* d_b, const double* d_x, double* d_r);
+
+/* ------------------------------------------------------------------- FSAI
+ * FSAI(const ptree&, shared_ptr<CSR>) of precond/FSAI/FSAI.hpp:14-37:
+ * optional filtered copy (filter_proper(tol_rel), then filter(tol_abs),
+ * core/CSR.hpp:423-525), pattern = lower(A) (power 1) or lower(A^2)
+ * (power 2) (precond/FSAI/symbolic.tpp:101-176), one dense LU per row
+ * (numeric.tpp:59-133), D-scaling (diagonal.cpp:6-73), FU stored transposed
+ * (core/CSR.hpp:151-211).  precision: 64 or 32 (float32 factor values for
+ * the apply; the setup always computes in float64). */
+int deco_fsai_create(deco_ctx ctx, deco_csr A, double tol_rel, double tol_abs, int power, int precision,
+                     deco_fsai* out);
+int deco_fsai_destroy(deco_fsai F);
+int deco_fsai_info(deco_fsai F, int* n, int* nz, int* max_order);
+/* FL (lower, diagonal last) and FU^T (upper) in the reference's layout. */
+int deco_fsai_download(deco_ctx ctx, deco_fsai F, int* h_Lr, int* h_Lc, double* h_Lv, int* h_Ur, int* h_Uc,
+                       double* h_Uv);
+/* y = FU^T (FL x)  (FSAI::precond, FSAI.hpp:40-47).  d_x may equal d_y. */
+int deco_fsai_apply(deco_ctx ctx, deco_fsai F, const double* d_x, double* d_y);
+
+/* -------------------------------------------------------------------- CPR
+ * CPR<int,int,double,Mglobal,Mlocal>(const ptree& prec, shared_ptr<CSR> A, V*& b)
+ * of precond/CPR.hpp:42-172.  Mutates A and d_b in place exactly as the
+ * reference (fix_diag, weights, row scaling, optional DRS, IMPES, CPD,
+ * optional zero filter, A_pp extraction and filter, FSAI setups, fix_diag
+ * undone).  The fields mirror the JSON keys read there. */
+typedef struct deco_cpr_params {
+  int block_size;        /* prec.block_size (2 or 3)                         */
+  int pressure_id;       /* prec.pressure_id                                 */
+  int seq;               /* prec.seq: 0, 1 or 3                              */
+  int weights;           /* prec.weights: 0 none, 1 quasiimpes, 2 quasiimpes_GE */
+  int use_drs;           /* prec.use_drs                                     */
+  double drs_e_dd;       /* prec.drs.e_dd                                    */
+  double drs_e_ps;       /* prec.drs.e_ps                                    */
+  int cpd;               /* prec.CPD                                         */
+  double tol_zero;       /* prec.tol_zero                                    */
+  double glo_tol_rel, glo_tol_abs; int glo_power;  /* prec.prec_glo.{tol_rel,tol_abs,power} */
+  double loc_tol_rel, loc_tol_abs; int loc_power;  /* prec.prec_loc.{tol_rel,tol_abs,power} */
+  int precision;         /* 64: float64 preconditioner; 32: float32 factors,
+                            float32 A copy and float32 vectors inside the apply */
+} deco_cpr_params;
+
+int deco_cpr_create(deco_ctx ctx, deco_csr A, double* d_b, const deco_cpr_params* prm, deco_cpr* out);
+int deco_cpr_destroy(deco_cpr P);
+/* x = M^{-1} r with the configured sequence (apply_seq0/1/3, CPR.hpp:176-299). */
+int deco_cpr_apply(deco_ctx ctx, deco_cpr P, const double* d_r, double* d_x);
+/* Borrowed handles of the pressure matrix and the two FSAI factors
+ * (which = 0 global on A, 1 local on A_pp).  Valid while P lives. */
+int deco_cpr_pressure(deco_cpr P, deco_csr* Ap);
+int deco_cpr_fsai(deco_cpr P, int which, deco_fsai* F);
+/* Setup timings in milliseconds: [decoupling, A_pp extraction, FSAI global,
+ * FSAI local, total] (the reference's profiler nodes "decoupling",
+ * "get local matrix", "Global precond", "Local  precond", "Prec"). */
+int deco_cpr_timings(deco_cpr P, double* h_ms5);
+/* Number of diagonal entries fix_diag replaced (CPR.hpp:753-840). */
+int deco_cpr_fixed_diagonals(deco_cpr P, int* count);
+
+/* ------------------------------------------------------------------ solve
+ * SOL<R,C,V>(ptree sol, A, precond, b, x) of solver/SOL.hpp:19-39 with
+ * type rgmres (solver/rgmres.tpp) or lgmres (solver/lgmres.tpp).  The
+ * Arnoldi step is classical Gram-Schmidt with one reorthogonalisation
+ * (CGS2) instead of the reference's modified Gram-Schmidt.
+ * precision 64: float64 everywhere.  precision 32: float32 Krylov basis and
+ * inner SpMV with float64 dot accumulation, float64 Hessenberg/Givens and a
+ * float64 true residual and solution update at every restart (iterative
+ * refinement); requires a CPR built with precision 32. */
+typedef struct deco_sol_params {
+  int type;              /* 0 rgmres, 1 lgmres                               */
+  double reltol;         /* sol.reltol                                       */
+  int restart;           /* sol.restart                                      */
+  int itmax;             /* sol.itmax (total inner iterations)               */
+  int verbosity;         /* sol.verbosity                                    */
+  int precision;         /* 64 or 32                                         */
+  int use_x0;            /* 1: d_x holds the initial guess; 0: start at zero */
+} deco_sol_params;
+
+typedef struct deco_sol_result {
+  int iter;              /* inner iterations (SOL::iter)                     */
+  int flag;              /* 0 converged, 1 not converged (SOL::flag)          */
+  double res_abs;        /* final residual norm (SOL::res_abs)               */
+  double res_rel;        /* res_abs / ||b|| (SOL::res_rel)                   */
+  double t_solve_ms;     /* device time of the solve                         */
+  int restarts;          /* completed restart cycles                         */
+} deco_sol_result;
+
+/* Solves A x = b with preconditioner P (NULL: identity).  A and d_b are the
+ * (decoupled) system.  h_resvec (optional, host, itmax+1 doubles) receives
+ * the residual history |g_j|/||b|| that the reference computes
+ * (rgmres.tpp:61) but discards. */
+int deco_gmres_solve(deco_ctx ctx, deco_csr A, deco_cpr P, const double* d_b, double* d_x,
+                     const deco_sol_params* prm, deco_sol_result* res, double* h_resvec);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,77 @@
+"""The C++ host layer (deco_b200/host/deco.hpp) through its driver, deco_cpr_gpu,
+on parameter files in the reference's format and on its binary CSR files."""
+import json
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import cpr_json, sol_json
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DRIVER = os.path.join(ROOT, "deco_b200", "deco_cpr_gpu")
+
+
+def write_params(tmp_path, io, prec, sol, hardware="GPU"):
+    text = "{\n  // reference-style parameter file (comments are stripped)\n" + \
+        '  "IO": ' + json.dumps(io) + ',\n  "sol": ' + json.dumps(sol) + ',\n  "prec": ' + json.dumps(prec) + \
+        ',\n  "parallel": {"hardware": "' + hardware + '", "np": "1", "nranks": "1"}\n}\n'
+    p = tmp_path / "param.json"
+    p.write_text(text)
+    return str(p)
+
+
+def run(param, *extra):
+    out = subprocess.run([DRIVER, param, *extra], capture_output=True, text=True, timeout=600)
+    m = re.search(r"iteration count =\s+(\d+)", out.stdout)
+    r = re.search(r"residual = ([0-9.e+-]+)", out.stdout)
+    return out.returncode, (int(m.group(1)) if m else None), (float(r.group(1)) if r else None), out
+
+
+@pytest.mark.gpu
+def test_driver_synthetic_matches_oracle(tmp_path):
+    from deco_b200 import gen
+    from oracle import port
+    prec = cpr_json(2)
+    sol = sol_json()
+    param = write_params(tmp_path, {"format": "synthetic", "preset": "1", "seed": "1234"}, prec, sol)
+    rc, it, res, out = run(param)
+    assert rc == 0, out.stderr
+    s = gen.generate(gen.preset(1, 1234))
+    ref_it = port.Cpr(prec, s.r, s.c, s.v, s.b).solve(sol)["iter"]
+    assert abs(it - ref_it) <= max(1, 0.1 * ref_it) and res < 1e-8
+    assert "Global precond" in out.stdout and "Local  precond" in out.stdout
+
+
+@pytest.mark.gpu
+def test_driver_reads_reference_binary_files(tmp_path):
+    """IO/cpp_read.hpp:331-442 layout: int n, m, nz; r; c; v  and  int n; b."""
+    from deco_b200 import gen
+    s = gen.grid(10, 8, 5, bs=3, seed=4)
+    fa, fb = tmp_path / "A.bin", tmp_path / "b.bin"
+    with open(fa, "wb") as f:
+        np.array([s.n, s.n, s.nnz], np.int32).tofile(f)
+        s.r.tofile(f); s.c.tofile(f); s.v.tofile(f)
+    with open(fb, "wb") as f:
+        np.array([s.n], np.int32).tofile(f)
+        s.b.tofile(f)
+    io = {"file_A": str(fa), "file_b": str(fb), "format": "bin", "wfile_x": str(tmp_path / "x.bin")}
+    param = write_params(tmp_path, io, cpr_json(3), sol_json("lgmres"))
+    rc, it, res, out = run(param)
+    assert rc == 0, out.stderr
+    assert it > 0 and res < 1e-8
+    x = np.fromfile(tmp_path / "x.bin", dtype=np.float64, offset=4)
+    assert x.shape == (s.n,) and np.all(np.isfinite(x))
+    rc32, it32, res32, out32 = run(param, "--precision", "32")
+    assert rc32 == 0 and res32 < 1e-8, out32.stderr
+
+
+@pytest.mark.gpu
+def test_driver_rejects_cpu_only_preconditioners(tmp_path):
+    prec = cpr_json(2)
+    prec["prec_loc"] = {"type": "hypre_AMG", "tol_rel": "1e-4"}
+    param = write_params(tmp_path, {"format": "synthetic", "preset": "1"}, prec, sol_json())
+    rc, it, res, out = run(param)
+    assert rc == 3 and "hypre" in out.stderr

@@ -1,0 +1,74 @@
+"""Synthetic systems: the named shapes, the CSR layout the reference's block
+arithmetic needs, determinism."""
+import numpy as np
+import pytest
+
+from deco_b200 import gen
+
+
+@pytest.mark.parametrize("cfg,n,nnz", [(1, 64000, 870400), (5, 262144, 3604480), (3, 8000000, 111360000)])
+def test_named_shapes(cfg, n, nnz):
+    s = gen.generate(gen.preset(cfg))
+    assert s.n == n and s.nnz == nnz
+
+
+def test_config2_has_fault_connections():
+    p = gen.preset(2)
+    s = gen.generate(p)
+    assert s.n == 1500000
+    stencil_only = 9 * (7 * 500000 - 2 * (100 * 50 + 100 * 50 + 100 * 100))
+    assert s.nnz > stencil_only  # 1% long-range pairs add dense 3x3 blocks
+
+
+def layout_checks(s):
+    r, c, v = s.r, s.c, s.v
+    rows = np.repeat(np.arange(s.n), np.diff(r))
+    # sorted, unique columns inside every row
+    assert np.all((np.diff(c) > 0) | (np.diff(rows) != 0))
+    # diagonal present in every row
+    assert np.count_nonzero(c == rows) == s.n
+    # every row of a cell has the same column pattern (precond/CPR.hpp:484-492)
+    bs = s.bs
+    lens = np.diff(r)
+    assert np.all(lens.reshape(-1, bs) == lens.reshape(-1, bs)[:, :1])
+    for cell in (0, s.n // bs // 2, s.n // bs - 1):
+        base = c[r[cell * bs]:r[cell * bs + 1]]
+        for p in range(1, bs):
+            np.testing.assert_array_equal(c[r[cell * bs + p]:r[cell * bs + p + 1]], base)
+    # dense bs x bs blocks: columns come in complete cell groups
+    assert np.all(np.diff(r) % bs == 0)
+    assert np.all(c.reshape(-1, bs) // bs == (c.reshape(-1, bs) // bs)[:, :1])
+    assert np.all(np.isfinite(v)) and np.count_nonzero(v == 0.0) == 0
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(bs=3, fault_frac=0.05, layered=1), dict(n_channels=3, channel_contrast=1e4)])
+def test_layout(kw):
+    layout_checks(gen.grid(9, 7, 5, seed=3, **kw))
+
+
+def test_structurally_symmetric_pattern():
+    s = gen.grid(8, 6, 4, bs=3, seed=9, fault_frac=0.05)
+    rows = np.repeat(np.arange(s.n), np.diff(s.r))
+    a = set(zip(rows.tolist(), s.c.tolist()))
+    assert all((j, i) in a for (i, j) in a)
+
+
+def test_deterministic_and_seeded():
+    a = gen.grid(10, 8, 6, seed=21)
+    b = gen.grid(10, 8, 6, seed=21)
+    c = gen.grid(10, 8, 6, seed=22)
+    np.testing.assert_array_equal(a.v, b.v)
+    np.testing.assert_array_equal(a.b, b.b)
+    assert not np.array_equal(a.v, c.v)
+
+
+def test_rhs_uniform():
+    s = gen.generate(gen.preset(1))
+    assert s.b.min() >= 0.0 and s.b.max() < 1.0 and abs(s.b.mean() - 0.5) < 0.01
+
+
+def test_invalid_parameters_are_rejected():
+    p = gen.preset(1)
+    p.bs = 4
+    with pytest.raises(ValueError):
+        gen.generate(p)
