@@ -170,7 +170,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="only the per-kernel timings (for profiler captures on a smaller --config)")
+    ap.add_argument("--config", type=int, default=3, help="system preset (3 = the benchmark workload)")
     args = ap.parse_args()
+    global CONFIG
+    CONFIG = args.config
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
@@ -196,6 +201,7 @@ def main():
     torch.cuda.set_stream(st)
     s = make_system()
     n, nnz = s.n, s.nnz
+    PREC["block_size"] = str(s.bs)
     dev = lambda a: torch.from_numpy(a).cuda()
     r_d, c_d, v_d, b_d = dev(s.r), dev(s.c), dev(s.v), dev(s.b)
     pin = lambda a: torch.from_numpy(a).pin_memory()
@@ -224,12 +230,15 @@ def main():
         e1.synchronize()
         ms = e0.elapsed_time(e1)
         true_rel = (A.residual(b, S.x).norm() / b.norm()).item()
+        ph = P.timings()
         info = dict(ms=ms, iter=S.iter, flag=S.flag, res_rel=S.res_rel, true_rel=true_rel,
-                    setup_ms=P.timings()["Prec"], solve_ms=S.time_ms)
+                    setup_ms=ph["Prec"], solve_ms=S.time_ms, setup_phases_ms={k: round(v, 2) for k, v in ph.items()})
         del S, P, A, b
         return info
 
     def timed(bits, k, host=False):
+        if k == 0:
+            return 0.0, [dict(ms=0, iter=0, flag=-1, res_rel=0, true_rel=0, setup_ms=0, solve_ms=0)], 0.0, 0
         barrier()
         l0 = lib().deco_launch_count()
         t0 = time.perf_counter()
@@ -240,6 +249,8 @@ def main():
         ms = replicas.max_over_ranks(sum(i["ms"] for i in infos) / k, device="cuda")
         return ms, infos, wall, launches
 
+    if args.kernels_only:
+        args.warmup, args.steps, args.no_fp64, args.no_e2e, args.no_cpu_baseline = 0, 0, True, True, True
     for _ in range(args.warmup):
         step(32)
     clk = Clocks(local)
@@ -251,7 +262,8 @@ def main():
         ms64, info64, _, _ = timed(64, args.steps)
         fp64 = {"time_s": ms64 / 1e3, "iterations": info64[-1]["iter"], "true_rel_residual": info64[-1]["true_rel"],
                 "setup_ms": info64[-1]["setup_ms"], "solve_ms": info64[-1]["solve_ms"],
-                "ms_per_iteration": info64[-1]["solve_ms"] / max(1, info64[-1]["iter"])}
+                "ms_per_iteration": info64[-1]["solve_ms"] / max(1, info64[-1]["iter"]),
+                "step_ms": [round(i["ms"], 1) for i in info64], "setup_phases_ms": info64[-1]["setup_phases_ms"]}
     e2e = None
     if not args.no_e2e:
         step(32, host=True)
@@ -334,7 +346,8 @@ def main():
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "mixed": {"iterations": last["iter"], "true_rel_residual": last["true_rel"], "flag": last["flag"],
                   "setup_ms": last["setup_ms"], "solve_ms": last["solve_ms"],
-                  "ms_per_iteration": last["solve_ms"] / max(1, last["iter"])},
+                  "ms_per_iteration": last["solve_ms"] / max(1, last["iter"]),
+                  "step_ms": [round(i["ms"], 1) for i in info_mixed], "setup_phases_ms": last.get("setup_phases_ms")},
         "fp64": fp64,
         "speedup_mixed_vs_fp64": (fp64["time_s"] / (ms_mixed / 1e3)) if fp64 else None,
         "gpu_launches": launches,

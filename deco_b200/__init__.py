@@ -140,7 +140,9 @@ class CSR:
 
     def apply_f32(self, x, b=None, bs: int = 1):
         torch = _torch()
-        check(lib().deco_csr_make_f32(self.ctx.h, self.h))
+        if not getattr(self, "_f32_ready", False):
+            check(lib().deco_csr_make_f32(self.ctx.h, self.h))
+            self._f32_ready = True
         x = _dev(x, torch.float32)
         if b is None:
             b = torch.empty((self.n + bs - 1) // bs, dtype=torch.float32, device="cuda")

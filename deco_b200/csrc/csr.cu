@@ -1,6 +1,9 @@
 // csr.cu — device CSR matrices (deco_csr), the SpMV autotuner and the SpMV /
 // residual entry points of the C ABI.
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "spmv.cuh"
 
@@ -40,12 +43,23 @@ void make_f32_values(deco_ctx_s* ctx, deco_csr_s* A) {
   DECO_CHECK_LAUNCH();
 }
 
+// process-wide cache of tuned widths, keyed by the matrix's shape, so a freshly
+// assembled system with the same structure is not timed again
+static std::map<std::tuple<int, int, int, int, bool>, int> g_tuned;
+static std::mutex g_tuned_mu;
+
 int tuned_subwarp(deco_ctx_s* ctx, deco_csr_s* A, bool f32) {
   int& sw = f32 ? A->sw32 : A->sw64;
   if (sw) return sw;
   const int W = f32 ? 4 : 2;
   sw = heuristic_subwarp(A->avg_row, W);
   if (!ctx->autotune || A->n < 4096) return sw;
+  const auto key = std::make_tuple(A->n, A->m, A->nz, A->max_row, f32);
+  {
+    std::lock_guard<std::mutex> lk(g_tuned_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) return sw = it->second;
+  }
   cudaStreamCaptureStatus cs;
   DECO_CUDA(cudaStreamIsCapturing(ctx->stream, &cs));
   if (cs != cudaStreamCaptureStatusNone) return sw;
@@ -77,6 +91,8 @@ int tuned_subwarp(deco_ctx_s* ctx, deco_csr_s* A, bool f32) {
     if (tot < best) { best = tot; best_sw = cand; }
   }
   sw = best_sw;
+  std::lock_guard<std::mutex> lk(g_tuned_mu);
+  g_tuned[key] = sw;
   return sw;
 }
 

@@ -110,10 +110,18 @@ __global__ void class_hist(int n, const int* __restrict__ fr, int* __restrict__ 
   if (threadIdx.x < 5 && h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
 }
 
+// warp-aggregated: lanes of one class share a single atomic on the class cursor
 __global__ void class_scatter(int n, const int* __restrict__ fr, int* __restrict__ cursor, int* __restrict__ perm) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    int cl = order_class(fr[i + 1] - fr[i] - 1);
-    if (cl >= 1 && cl <= 3) perm[atomicAdd(&cursor[cl], 1)] = i;
+  const int lane = threadIdx.x & 31;
+  for (int base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; base < n; base += gridDim.x * blockDim.x) {
+    const int i = base + lane;
+    const int cl = i < n ? order_class(fr[i + 1] - fr[i] - 1) : 0;
+    const unsigned same = __match_any_sync(0xffffffffu, cl);
+    const int leader = __ffs(same) - 1;
+    int pos = 0;
+    if (lane == leader && cl >= 1 && cl <= 3) pos = atomicAdd(&cursor[cl], __popc(same));
+    pos = __shfl_sync(0xffffffffu, pos, leader) + __popc(same & ((1u << lane) - 1));
+    if (i < n && cl >= 1 && cl <= 3) perm[pos] = i;
   }
 }
 

@@ -1,21 +1,26 @@
 // gmres.cu — restarted right / left preconditioned GMRES(m) on the device
 // (solver/rgmres.tpp:8-139, solver/lgmres.tpp:1-134; Givens :141-160).
 //
-// Arnoldi step: classical Gram-Schmidt with one reorthogonalisation (CGS2) in
-// three fused passes over the basis V (column-major, one column per vector):
-//   pass A   h  = V^T w                                  (dots)
-//   pass B   w' = w - V h;  h2 = V^T w';  s = ||w'||^2   (update + dots; the
-//            second read of each V tile hits L2)
-//            the block that finishes last reduces the partial sums, forms
-//            H(:,j) = h + h2, beta = sqrt(s - ||h2||^2) (w'' = w' - V h2 is
-//            orthogonal to V, so Pythagoras gives its norm without a pass),
-//            and applies the Givens rotations to H(:,j) and g — on the device;
-//   pass C   v_{j+1} = (w' - V h2) / beta.
-// Only |g_{j+1}| (8 bytes) returns to the host per iteration.  The reference
-// uses modified Gram-Schmidt (rgmres.tpp:72-75): 5(j+1) vector passes per
-// step against 3(j+1)+5 here.
+// Arnoldi step: classical Gram-Schmidt with reorthogonalisation (CGS2) in two
+// passes over the basis, the second projection taken from the Gram matrix
+// instead of a second dot pass:
+//   pass A   one read of V computes  h = V^T w  and the new Gram row  V^T v_j.
+//            The block that finishes last forms G (the Gram matrix of the
+//            stored basis), the reorthogonalisation h2 = V^T (w - V h) =
+//            h - G h, and the coefficients c = h + h2, which leave (I - G)^2 of
+//            the orthogonality defect, as CGS2 does.
+//   pass B   w'' = w - V c, written as the next basis column, and ||w''||^2.
+//            The last block sets H(:,j) = c, H(j+1,j) = ||w''|| and applies the
+//            Givens rotations (the reference's formulas) on the device.
+// Normalisation is lazy: column k is stored unnormalised with a scale s_k that
+// the next SpMV epilogue, the coefficients and the combination absorb, so no
+// pass is spent on scaling.  Per iteration the basis is read twice (the
+// reference's modified Gram-Schmidt, rgmres.tpp:72-75, reads it 2(j+1) times and
+// w 3(j+1) times).  |g_{j+1}| returns to the host one iteration behind: the next
+// iteration is already queued when the host checks convergence, so the device
+// does not wait on the host.
 //
-// Precision 32: V, w, z in float32 with float64 dot accumulation; H, g and the
+// Precision 32: V, w, z in float32 with float64 accumulation; H, G, g and the
 // rotations in float64; every restart recomputes the true residual b - A x and
 // the solution update in float64 (iterative refinement).
 #include <cmath>
@@ -30,16 +35,33 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kColsPerWarp = 8;
-constexpr int kMaxCols = kWarps * kColsPerWarp;  // basis columns the CGS kernels handle (restart <= 63)
+constexpr int kMaxCols = kWarps * kColsPerWarp;  // basis columns pass A handles (restart <= 63)
+constexpr int kRowsPerLane = 8;                   // rows per lane per step of pass A
 constexpr double kEps = 2.220446049250312e-16;
 
-// st layout (float64): H (m+1)*m | g | cs | sn | hA | hB (m+1 each) | sc[16]
+// device state (float64): H (m+1)*m | G (m+1)^2 | g | cs | sn | s | c | sums 2(m+2) | sc
 struct State {
-  double* H; double* g; double* cs; double* sn; double* hA; double* hB; double* sc;
+  double* H; double* G; double* g; double* cs; double* sn; double* s; double* c; double* sums; double* sc;
   int m;
   __host__ __device__ double& h(int i, int j) const { return H[i + (size_t)j * (m + 1)]; }
+  __host__ __device__ double& gm(int i, int j) const { return G[i + (size_t)j * (m + 1)]; }
+  static size_t doubles(int m) {
+    return (size_t)(m + 1) * m + (size_t)(m + 1) * (m + 1) + 5 * (size_t)(m + 1) + 2 * (size_t)(m + 2) + 16;
+  }
+  void bind(double* b, int m_) {
+    m = m_;
+    H = b;
+    G = H + (size_t)(m + 1) * m;
+    g = G + (size_t)(m + 1) * (m + 1);
+    cs = g + (m + 1);
+    sn = cs + (m + 1);
+    s = sn + (m + 1);
+    c = s + (m + 1);
+    sums = c + (m + 1);
+    sc = sums + 2 * (m + 2);
+  }
 };
-enum { SC_SS = 0, SC_BETA = 1, SC_INVB = 2, SC_RES = 3, SC_BREAK = 4, SC_NORM = 5, SC_INVN = 6 };
+enum { SC_RES = 0, SC_BREAK = 1, SC_BETA = 2 };
 
 __device__ __forceinline__ double ldv(const double* p) { return __ldcs(p); }
 __device__ __forceinline__ double ldv(const float* p) { return (double)__ldcs(p); }
@@ -55,6 +77,7 @@ __device__ void finalize_partials(const double* red, int nb, int ncols, double* 
   }
 }
 
+// true in the block that finishes last (no waiting: an atomic ticket)
 __device__ __forceinline__ bool last_block(unsigned* counter) {
   __shared__ bool amlast;
   __threadfence();
@@ -64,60 +87,17 @@ __device__ __forceinline__ bool last_block(unsigned* counter) {
   return amlast;
 }
 
-// warp-reduce v and add it to acc[i*kWarps + warp]
-__device__ __forceinline__ void acc_add(double* acc, int i, double v) {
+__device__ void block_sum_to(double v, double* red_slot) {
+  __shared__ double part[kWarps];
   v = warp_sum(v);
-  if ((threadIdx.x & 31) == 0) acc[i * kWarps + (threadIdx.x >> 5)] += v;
-}
-
-__device__ void flush_acc(double* acc, int ncols, double* red) {
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
   __syncthreads();
-  for (int i = threadIdx.x; i < ncols; i += kThreads) {
-    double s = 0.0;
+  if (threadIdx.x == 0) {
+    double t = 0.0;
 #pragma unroll
-    for (int w = 0; w < kWarps; ++w) s += acc[i * kWarps + w];
-    red[(size_t)i * gridDim.x + blockIdx.x] = s;
+    for (int k = 0; k < kWarps; ++k) t += part[k];
+    *red_slot = t;
   }
-}
-
-// ---- pass A: hA[i] = V_i . w, i < ncols.  Warp w owns columns w, w+8, ...;
-// its lanes stride over rows and keep one partial sum per owned column in
-// registers for the whole kernel, so every column is reduced once per block.
-// The block's tile of w is staged in shared memory and shared by the warps.
-template <typename T, int KPW>
-__global__ void __launch_bounds__(kThreads) cgs_pass_a(long long n, long long ld, int ncols, const T* __restrict__ V,
-                                                       const T* __restrict__ w, double* __restrict__ red,
-                                                       unsigned* counter, double* __restrict__ hA) {
-  __shared__ double ws[kThreads];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double p[KPW];
-#pragma unroll
-  for (int k = 0; k < KPW; ++k) p[k] = 0.0;
-  for (long long base = (long long)blockIdx.x * kThreads; base < n; base += (long long)gridDim.x * kThreads) {
-    const long long r = base + threadIdx.x;
-    ws[threadIdx.x] = r < n ? (double)w[r] : 0.0;
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < KPW; ++k) {
-      const int c = warp + k * kWarps;
-      if (c < ncols) {
-        const T* vc = V + (size_t)c * ld + base;
-#pragma unroll
-        for (int q = 0; q < kThreads / 32; ++q) {
-          const int t = lane + 32 * q;
-          if (base + t < n) p[k] += ldv(vc + t) * ws[t];
-        }
-      }
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int k = 0; k < KPW; ++k) {
-    const int c = warp + k * kWarps;
-    const double t = warp_sum(p[k]);
-    if (lane == 0 && c < ncols) red[(size_t)c * gridDim.x + blockIdx.x] = t;
-  }
-  if (last_block(counter)) finalize_partials(red, gridDim.x, ncols, hA);
 }
 
 __device__ void givens_make(double x, double y, double& c, double& s) {
@@ -131,87 +111,105 @@ __device__ void givens_apply(double c, double s, double& dx, double& dy) {
   dx = t;
 }
 
-// ---- pass B: w' = w - V hA (in place), hB = V^T w', ss = ||w'||^2.  Each
-// block tile of kThreads rows x ncols columns is read once from HBM into
-// shared memory while the update runs; the second dot product then reads the
-// tile from shared memory, warp w owning columns w, w+8, ... with per-lane
-// partials in registers.  The last block finalises column j of H and the
-// Givens rotations.
-template <typename T, int KPW>
-__global__ void __launch_bounds__(kThreads) cgs_pass_b(long long n, long long ld, int ncols, const T* __restrict__ V,
-                                                       T* __restrict__ w, double* __restrict__ red, unsigned* counter,
-                                                       State st, int j) {
-  extern __shared__ unsigned char smraw[];
-  double* hs = reinterpret_cast<double*>(smraw);            // ncols coefficients
-  double* ws = hs + kMaxCols;                                // kThreads updated w'
-  T* Vs = reinterpret_cast<T*>(ws + kThreads);               // ncols x kThreads tile
-  __shared__ double ssw[kWarps];
+// ---- pass A: raw dots u_c . w and u_c . u_j for c < ncols (u = stored columns).
+// Blocks own contiguous row ranges; warp w owns columns w, w+8, ...; lanes keep
+// per-column partial sums in registers for the whole range (no barriers).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long ld, int ncols, int j,
+                                                         const T* __restrict__ V, const T* __restrict__ w,
+                                                         double* __restrict__ red, unsigned* counter, State st) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int i = threadIdx.x; i < ncols; i += kThreads) hs[i] = st.hA[i];
-  __syncthreads();
-  double p[KPW];
+  const T* __restrict__ uj = V + (size_t)j * ld;
+  const long long per = (n + gridDim.x - 1) / gridDim.x;
+  const long long r0 = per * blockIdx.x, r1 = min(n, r0 + per);
+  double pw[kColsPerWarp], pu[kColsPerWarp];
 #pragma unroll
-  for (int k = 0; k < KPW; ++k) p[k] = 0.0;
-  double ss = 0.0;
-  for (long long base = (long long)blockIdx.x * kThreads; base < n; base += (long long)gridDim.x * kThreads) {
-    const long long r = base + threadIdx.x;
-    if (r < n) {
-      double x = (double)w[r];
-#pragma unroll 8
-      for (int i = 0; i < ncols; ++i) {
-        const T v = __ldcs(V + (size_t)i * ld + r);
-        Vs[i * kThreads + threadIdx.x] = v;
-        x -= hs[i] * (double)v;
-      }
-      const T xq = (T)x;
-      w[r] = xq;
-      ws[threadIdx.x] = (double)xq;
-      ss += (double)xq * (double)xq;
-    } else {
-      for (int i = 0; i < ncols; ++i) Vs[i * kThreads + threadIdx.x] = (T)0;
-      ws[threadIdx.x] = 0.0;
+  for (int k = 0; k < kColsPerWarp; ++k) { pw[k] = 0.0; pu[k] = 0.0; }
+  constexpr int step = 32 * kRowsPerLane;
+  for (long long base = r0; base < r1; base += step) {
+    double wv[kRowsPerLane], uv[kRowsPerLane];
+#pragma unroll
+    for (int q = 0; q < kRowsPerLane; ++q) {
+      const long long r = base + lane + 32 * q;
+      const bool ok = r < r1;
+      wv[q] = ok ? (double)w[r] : 0.0;
+      uv[q] = ok ? (double)uj[r] : 0.0;
     }
-    __syncthreads();
 #pragma unroll
-    for (int k = 0; k < KPW; ++k) {
+    for (int k = 0; k < kColsPerWarp; ++k) {
       const int c = warp + k * kWarps;
       if (c < ncols) {
-        const T* vc = Vs + c * kThreads;
+        const T* __restrict__ vc = V + (size_t)c * ld;
 #pragma unroll
-        for (int q = 0; q < kThreads / 32; ++q) p[k] += (double)vc[lane + 32 * q] * ws[lane + 32 * q];
+        for (int q = 0; q < kRowsPerLane; ++q) {
+          const long long r = base + lane + 32 * q;
+          if (r < r1) {
+            const double v = ldv(vc + r);
+            pw[k] += v * wv[q];
+            pu[k] += v * uv[q];
+          }
+        }
       }
     }
-    __syncthreads();
   }
 #pragma unroll
-  for (int k = 0; k < KPW; ++k) {
+  for (int k = 0; k < kColsPerWarp; ++k) {
     const int c = warp + k * kWarps;
-    const double t = warp_sum(p[k]);
-    if (lane == 0 && c < ncols) red[(size_t)c * gridDim.x + blockIdx.x] = t;
-  }
-  ss = warp_sum(ss);
-  if (lane == 0) ssw[warp] = ss;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-#pragma unroll
-    for (int k = 0; k < kWarps; ++k) t += ssw[k];
-    red[(size_t)ncols * gridDim.x + blockIdx.x] = t;
+    const double a = warp_sum(pw[k]), b = warp_sum(pu[k]);
+    if (lane == 0 && c < ncols) {
+      red[(size_t)c * gridDim.x + blockIdx.x] = a;
+      red[(size_t)(ncols + c) * gridDim.x + blockIdx.x] = b;
+    }
   }
   if (!last_block(counter)) return;
-  finalize_partials(red, gridDim.x, ncols + 1, st.hB);
+  finalize_partials(red, gridDim.x, 2 * ncols, st.sums);
+  __syncthreads();
+  // h_i = s_i (u_i . w);  G(i,j) = s_i s_j (u_i . u_j)
+  double* h = st.sums;  // scaled in place
+  const double sj = st.s[j];
+  for (int i = threadIdx.x; i < ncols; i += kThreads) {
+    h[i] *= st.s[i];
+    const double gij = st.s[i] * sj * st.sums[ncols + i];
+    st.gm(i, j) = gij;
+    st.gm(j, i) = gij;
+  }
+  __syncthreads();
+  // c = h + (h - G h): the second Gram-Schmidt projection from the Gram matrix
+  for (int i = threadIdx.x; i < ncols; i += kThreads) {
+    double gh = 0.0;
+    for (int k = 0; k < ncols; ++k) gh += st.gm(i, k) * h[k];
+    const double ci = h[i] + (h[i] - gh);
+    st.h(i, j) = ci;
+    st.c[i] = ci * st.s[i];  // coefficient on the stored (unnormalised) column
+  }
+}
+
+// ---- pass B: w'' = w - sum_c coef_c u_c, stored as column j+1; ||w''||^2
+template <typename T>
+__global__ void __launch_bounds__(kThreads) arnoldi_update(long long n, long long ld, int ncols, int j,
+                                                           const T* __restrict__ V, const T* __restrict__ w,
+                                                           T* __restrict__ out, double* __restrict__ red,
+                                                           unsigned* counter, State st) {
+  __shared__ double cs_[kMaxCols];
+  for (int i = threadIdx.x; i < ncols; i += kThreads) cs_[i] = st.c[i];
+  __syncthreads();
+  double ss = 0.0;
+  for (long long r = (long long)blockIdx.x * kThreads + threadIdx.x; r < n; r += (long long)gridDim.x * kThreads) {
+    double x = (double)w[r];
+#pragma unroll 8
+    for (int i = 0; i < ncols; ++i) x -= cs_[i] * ldv(V + (size_t)i * ld + r);
+    const T xq = (T)x;
+    out[r] = xq;
+    ss += (double)xq * (double)xq;
+  }
+  block_sum_to(ss, red + blockIdx.x);
+  if (!last_block(counter)) return;
+  finalize_partials(red, gridDim.x, 1, st.sc + SC_BETA);
   __syncthreads();
   if (threadIdx.x == 0) {
-    double ssum = st.hB[ncols], h2n = 0.0;
-    for (int i = 0; i < ncols; ++i) {
-      st.h(i, j) = st.hA[i] + st.hB[i];
-      h2n += st.hB[i] * st.hB[i];
-    }
-    double b2 = ssum - h2n;
-    double beta = b2 > 0.0 ? sqrt(b2) : 0.0;
+    const double beta = sqrt(st.sc[SC_BETA]);
     st.h(j + 1, j) = beta;
-    st.sc[SC_BETA] = beta;
-    st.sc[SC_INVB] = beta != 0.0 ? 1.0 / beta : 0.0;
+    st.s[j + 1] = beta != 0.0 ? 1.0 / beta : 0.0;
     for (int i = 0; i <= j - 1; ++i) givens_apply(st.cs[i], st.sn[i], st.h(i, j), st.h(i + 1, j));
     givens_make(st.h(j, j), st.h(j + 1, j), st.cs[j], st.sn[j]);
     givens_apply(st.cs[j], st.sn[j], st.h(j, j), st.h(j + 1, j));
@@ -220,58 +218,69 @@ __global__ void __launch_bounds__(kThreads) cgs_pass_b(long long n, long long ld
   }
 }
 
+// ---- column 0: u_0 = r, s_0 = 1/||r||, g_0 = ||r|| (rgmres.tpp:54-55); out[0] = ||r||
 template <typename T>
-size_t pass_b_smem(int ncols) { return (size_t)(kMaxCols + kThreads) * sizeof(double) + (size_t)ncols * kThreads * sizeof(T); }
-
-// ---- pass C: v_{j+1} = (w' - V hB) / beta
-template <typename T>
-__global__ void __launch_bounds__(kThreads) cgs_pass_c(long long n, long long ld, int ncols, const T* __restrict__ V,
-                                                       const T* __restrict__ w, State st, T* __restrict__ vout) {
-  const double inv = st.sc[SC_INVB];
-  for (long long r = (long long)blockIdx.x * kThreads + threadIdx.x; r < n; r += (long long)gridDim.x * kThreads) {
-    double x = (double)w[r];
-    for (int i = 0; i < ncols; ++i) x -= st.hB[i] * (double)__ldcs(V + (size_t)i * ld + r);
-    vout[r] = (T)(x * inv);
+__global__ void __launch_bounds__(kThreads) start_cycle(long long n, const double* __restrict__ r, T* __restrict__ u0,
+                                                        double* __restrict__ red, unsigned* counter, State st,
+                                                        double* __restrict__ out) {
+  double ss = 0.0, sq = 0.0;
+  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n; i += (long long)gridDim.x * kThreads) {
+    const double v = r[i];
+    const T vq = (T)v;
+    u0[i] = vq;
+    ss += v * v;
+    sq += (double)vq * (double)vq;
   }
-}
-
-// ---- norms, scaling, combination
-template <typename T>
-__global__ void __launch_bounds__(kThreads) sumsq(long long n, const T* __restrict__ x, double* __restrict__ red,
-                                                  unsigned* counter, double* __restrict__ out) {
-  extern __shared__ double acc[];
-  for (int t = threadIdx.x; t < kWarps; t += kThreads) acc[t] = 0.0;
+  block_sum_to(ss, red + blockIdx.x);
+  block_sum_to(sq, red + gridDim.x + blockIdx.x);
+  if (!last_block(counter)) return;
+  finalize_partials(red, gridDim.x, 2, out);
   __syncthreads();
-  double s = 0.0;
-  for (long long r = (long long)blockIdx.x * kThreads + threadIdx.x; r < n; r += (long long)gridDim.x * kThreads) {
-    double v = (double)x[r];
-    s += v * v;
-  }
-  acc_add(acc, 0, s);
-  flush_acc(acc, 1, red);
-  if (last_block(counter)) {
-    finalize_partials(red, gridDim.x, 1, out);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      out[0] = sqrt(out[0]);
-      out[1] = 1.0 / out[0];  // reference: axpby(n, 1/g[0], r, v0)
-    }
+  if (threadIdx.x == 0) {
+    const double nrm = sqrt(out[0]), nq = sqrt(out[1]);
+    out[0] = nrm;
+    st.g[0] = nrm;
+    st.s[0] = nq != 0.0 ? 1.0 / nq : 0.0;  // scale of the stored column
   }
 }
 
-template <typename S, typename T>
-__global__ void scale_into(long long n, const S* __restrict__ x, const double* __restrict__ factor, T* __restrict__ y) {
-  const double f = *factor;
-  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x)
-    y[r] = (T)(f * (double)x[r]);
+// ---- ||x||_2 in float64, deterministic
+template <typename X>
+__global__ void __launch_bounds__(kThreads) norm2_kernel(long long n, const X* __restrict__ x, double* __restrict__ red,
+                                                         unsigned* counter, double* __restrict__ out) {
+  double ss = 0.0;
+  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n; i += (long long)gridDim.x * kThreads) {
+    const double v = (double)x[i];
+    ss += v * v;
+  }
+  block_sum_to(ss, red + blockIdx.x);
+  if (!last_block(counter)) return;
+  finalize_partials(red, gridDim.x, 1, out);
+  __syncthreads();
+  if (threadIdx.x == 0) out[0] = sqrt(out[0]);
 }
 
+// back substitution g(1:j) = H(1:j,1:j) \ g(1:j)  (rgmres.tpp:95-104), then the
+// coefficients on the stored columns c_i = y_i s_i
+__global__ void backsolve(State st, int j) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  st.sc[SC_BREAK] = 0.0;
+  for (int i = j - 1; i >= 0; --i) {
+    if (st.h(i, i) == 0.0) { st.sc[SC_BREAK] = 1.0; return; }
+    st.g[i] /= st.h(i, i);
+    for (int k = 0; k < i; ++k) st.g[k] -= st.h(k, i) * st.g[i];
+  }
+  const int nc = j > 0 ? j : 1;
+  for (int i = 0; i < nc; ++i) st.c[i] = st.g[i] * st.s[i];
+}
+
+// out = sum_{i < ncols} c_i u_i  (rgmres.tpp:106-109: w = g_0 v_0, then w += g_i v_i)
 template <typename T, typename Y>
-__global__ void combine(long long n, long long ld, int ncols, const T* __restrict__ V, const double* __restrict__ y,
+__global__ void combine(long long n, long long ld, int ncols, const T* __restrict__ V, const double* __restrict__ c,
                         Y* __restrict__ out) {
   for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
-    double s = y[0] * (double)V[r];
-    for (int i = 1; i < ncols; ++i) s = 1.0 * s + y[i] * (double)V[(size_t)i * ld + r];
+    double s = c[0] * (double)V[r];
+    for (int i = 1; i < ncols; ++i) s += c[i] * (double)V[(size_t)i * ld + r];
     out[r] = (Y)s;
   }
 }
@@ -282,23 +291,11 @@ __global__ void axpy_into(long long n, const X* __restrict__ z, double* __restri
     x[r] += (double)z[r];
 }
 
-// back substitution g(1:j) = H(1:j,1:j) \ g(1:j)  (rgmres.tpp:95-104)
-__global__ void backsolve(State st, int j) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  st.sc[SC_BREAK] = 0.0;
-  for (int i = j - 1; i >= 0; --i) {
-    if (st.h(i, i) == 0.0) { st.sc[SC_BREAK] = 1.0; return; }
-    st.g[i] /= st.h(i, i);
-    for (int k = 0; k < i; ++k) st.g[k] -= st.h(k, i) * st.g[i];
-  }
-}
-
-__global__ void set_g0(State st, const double* norm) { st.g[0] = norm[0]; }
-
 template <typename S, typename D>
-__global__ void convert(long long n, const S* __restrict__ a, D* __restrict__ b) {
+__global__ void scale_convert(long long n, const S* __restrict__ a, const double* __restrict__ s, D* __restrict__ b) {
+  const double f = s ? __ldg(s) : 1.0;
   for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x)
-    b[r] = (D)a[r];
+    b[r] = (D)(f * (double)a[r]);
 }
 
 // ------------------------------------------------------------------ driver
@@ -319,37 +316,27 @@ struct Solver {
     n = A->n;
     ld = (n + 31) / 32 * 32;
     m = prm.restart;
-    nb = 2 * ctx->num_sms;
+    nb = 4 * ctx->num_sms;
     cudaStream_t s = ctx->stream;
     V.alloc((size_t)ld * (m + 1), s);
     w.alloc(n, s);
     z.alloc(n, s);
-    st_buf.alloc((size_t)(m + 1) * m + 5 * (m + 1) + 16, s);
+    st_buf.alloc(State::doubles(m), s);
+    st.bind(st_buf.get(), m);
     xtmp.alloc(n, s);
     r64.alloc(n, s);
     norm.alloc(4, s);
-    double* b = st_buf.get();
-    st.m = m;
-    st.H = b;
-    st.g = b + (size_t)(m + 1) * m;
-    st.cs = st.g + (m + 1);
-    st.sn = st.cs + (m + 1);
-    st.hA = st.sn + (m + 1);
-    st.hB = st.hA + (m + 1);
-    st.sc = st.hB + (m + 1);
-    size_t need = (size_t)(m + 2) * nb;
+    const size_t need = (size_t)(2 * (m + 2)) * nb;
     if (ctx->red.size() < need) ctx->red.alloc(need, s);
-    DECO_CUDA(cudaFuncSetAttribute(cgs_pass_b<T, kColsPerWarp>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)pass_b_smem<T>(kMaxCols)));
   }
 
-  int grid() const { return nb; }
+  T* col(int i) { return V.get() + (size_t)i * ld; }
 
   // y = M^{-1} x
   template <typename X, typename Y>
   void precond(const X* x, Y* y) {
     if (!P) {
-      convert<X, Y><<<grid(), kThreads, 0, ctx->stream>>>(n, x, y);
+      scale_convert<X, Y><<<nb, kThreads, 0, ctx->stream>>>(n, x, nullptr, y);
       DECO_CHECK_LAUNCH();
       return;
     }
@@ -364,17 +351,15 @@ struct Solver {
     }
   }
 
-  // y = A x in the basis precision
+  // y = s * (A x) in the basis precision, s on the device
   template <typename X>
-  void matvec(const X* x, T* y) {
-    if constexpr (std::is_same<T, float>::value) spmv<float, X>(ctx, A, x, EpiStore<float>{y});
-    else spmv<double, X>(ctx, A, x, EpiStore<double>{y});
+  void matvec_scaled(const X* x, T* y, const double* s) {
+    if constexpr (std::is_same<T, float>::value) spmv<float, X>(ctx, A, x, EpiStoreScaled<float>{y, s});
+    else spmv<double, X>(ctx, A, x, EpiStoreScaled<double>{y, s});
   }
 
-  template <typename X>
-  double norm2(const X* x) {
-    size_t sm = kWarps * sizeof(double);
-    sumsq<X><<<grid(), kThreads, sm, ctx->stream>>>(n, x, ctx->red.get(), ctx->counter.get(), norm.get());
+  double norm2(const double* x) {
+    norm2_kernel<double><<<nb, kThreads, 0, ctx->stream>>>(n, x, ctx->red.get(), ctx->counter.get(), norm.get());
     DECO_CHECK_LAUNCH();
     double h = 0;
     DECO_CUDA(cudaMemcpyAsync(&h, norm.get(), sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -382,16 +367,35 @@ struct Solver {
     return h;
   }
 
-  T* col(int i) { return V.get() + (size_t)i * ld; }
+  // Arnoldi step j: writes column j of H/G, g_{j+1}, rotation j and basis column
+  // j+1; |g_{j+1}| is copied to host slot (j & 1) and ev[j & 1] recorded after it.
+  void arnoldi_step(int j, bool left, volatile double* hsc, cudaEvent_t* ev) {
+    cudaStream_t s = ctx->stream;
+    const double* sj = st.s + j;
+    if (!left) {
+      precond<T, T>(col(j), z.get());
+      matvec_scaled<T>(z.get(), w.get(), sj);
+    } else {
+      matvec_scaled<T>(col(j), z.get(), sj);
+      precond<T, T>(z.get(), w.get());
+    }
+    const int nc = j + 1;
+    arnoldi_dots<T><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V.get(), w.get(), ctx->red.get(), ctx->counter.get(), st);
+    DECO_CHECK_LAUNCH();
+    arnoldi_update<T><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V.get(), w.get(), col(j + 1), ctx->red.get(),
+                                              ctx->counter.get(), st);
+    DECO_CHECK_LAUNCH();
+    DECO_CUDA(cudaMemcpyAsync(const_cast<double*>(hsc) + (j & 1), st.sc + SC_RES, sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+    DECO_CUDA(cudaEventRecord(ev[j & 1], s));
+  }
 
   void run(const double* b, double* x, deco_sol_result* res, double* resvec) {
     cudaStream_t s = ctx->stream;
     const bool left = prm.type == 1;
     const int itmax = prm.itmax;
-    const int g = grid();
     double* r = r64.get();
     DECO_CUDA(cudaEventRecord(ctx->ev0, s));
-    // initial residual
     if (!prm.use_x0) {
       DECO_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, s));
       if (left) precond<double, double>(b, r);
@@ -404,56 +408,62 @@ struct Solver {
     const double abstol = prm.reltol * bnorm;
     int flag = 1, iter = 0, restarts = 0;
     double rnorm = 0.0;
-    double* hsc = ctx->host_scalars;
+    volatile double* hsc = ctx->host_scalars;
+    cudaEvent_t ev[2];
+    DECO_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    DECO_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    struct EvGuard {
+      cudaEvent_t* e;
+      ~EvGuard() { cudaEventDestroy(e[0]); cudaEventDestroy(e[1]); }
+    } evg{ev};
     while (iter < itmax) {
-      DECO_CUDA(cudaMemsetAsync(st_buf.get(), 0, sizeof(double) * ((size_t)(m + 1) * m + 5 * (m + 1) + 16), s));
-      double g0 = norm2(r);
-      set_g0<<<1, 1, 0, s>>>(st, norm.get());
-      scale_into<double, T><<<g, kThreads, 0, s>>>(n, r, norm.get() + 1, col(0));
+      DECO_CUDA(cudaMemsetAsync(st_buf.get(), 0, sizeof(double) * State::doubles(m), s));
+      start_cycle<T><<<nb, kThreads, 0, s>>>(n, r, col(0), ctx->red.get(), ctx->counter.get(), st, norm.get());
       DECO_CHECK_LAUNCH();
+      DECO_CUDA(cudaMemcpyAsync(const_cast<double*>(hsc) + 2, norm.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+      DECO_CUDA(cudaStreamSynchronize(s));
+      double gj = hsc[2];
+      bool known = true;  // |g_j| is on the host; otherwise it is in flight from step j-1
       int j = 0;
-      double gj = g0;
-      while (j < m && iter < itmax) {
-        rnorm = fabs(gj);
-        if (resvec) resvec[iter] = rnorm / bnorm;
-        if (rnorm < abstol) { flag = 0; break; }
-        if (!left) {
-          precond<T, T>(col(j), z.get());
-          matvec<T>(z.get(), w.get());
+      for (;;) {
+        // the reference's loop bounds and inner convergence check (rgmres.tpp:58-66)
+        if (!(j < m && iter < itmax)) break;
+        if (known) {
+          rnorm = fabs(gj);
+          if (resvec) resvec[iter] = rnorm / bnorm;
+          if (rnorm < abstol) { flag = 0; break; }
+          arnoldi_step(j, left, hsc, ev);
         } else {
-          matvec<T>(col(j), z.get());
-          precond<T, T>(z.get(), w.get());
+          // enqueue step j before looking at |g_j| from step j-1; if |g_j| already
+          // meets the tolerance, step j is dropped: it wrote only column j of H/G,
+          // g_{j+1}, rotation j and basis column j+1, which the back substitution
+          // over j columns never reads
+          arnoldi_step(j, left, hsc, ev);
+          DECO_CUDA(cudaEventSynchronize(ev[(j - 1) & 1]));
+          gj = hsc[(j - 1) & 1];
+          rnorm = fabs(gj);
+          if (resvec) resvec[iter] = rnorm / bnorm;
+          if (rnorm < abstol) { flag = 0; break; }
         }
-        const int nc = j + 1;
-        cgs_pass_a<T, kColsPerWarp><<<g, kThreads, 0, s>>>(n, ld, nc, V.get(), w.get(), ctx->red.get(),
-                                                           ctx->counter.get(), st.hA);
-        DECO_CHECK_LAUNCH();
-        cgs_pass_b<T, kColsPerWarp><<<g, kThreads, pass_b_smem<T>(nc), s>>>(n, ld, nc, V.get(), w.get(),
-                                                                           ctx->red.get(), ctx->counter.get(), st, j);
-        DECO_CHECK_LAUNCH();
-        cgs_pass_c<T><<<g * 4, kThreads, 0, s>>>(n, ld, nc, V.get(), w.get(), st, col(j + 1));
-        DECO_CHECK_LAUNCH();
-        DECO_CUDA(cudaMemcpyAsync(hsc, st.sc + SC_RES, sizeof(double), cudaMemcpyDeviceToHost, s));
-        DECO_CUDA(cudaStreamSynchronize(s));
-        gj = hsc[0];
         ++j;
         ++iter;
+        known = false;
       }
       backsolve<<<1, 1, 0, s>>>(st, j);
       DECO_CHECK_LAUNCH();
-      DECO_CUDA(cudaMemcpyAsync(hsc, st.sc + SC_BREAK, sizeof(double), cudaMemcpyDeviceToHost, s));
+      DECO_CUDA(cudaMemcpyAsync(const_cast<double*>(hsc) + 3, st.sc + SC_BREAK, sizeof(double), cudaMemcpyDeviceToHost, s));
       DECO_CUDA(cudaStreamSynchronize(s));
-      if (hsc[0] != 0.0)
+      if (hsc[3] != 0.0)
         throw Error(DECO_ERR_BREAKDOWN, "Error in rgmres: Zero diagonal element in upper triangular matrix.");
-      combine<T, double><<<g * 4, kThreads, 0, s>>>(n, ld, j > 0 ? j : 1, V.get(), st.g, xtmp.get());
+      combine<T, double><<<nb, kThreads, 0, s>>>(n, ld, j > 0 ? j : 1, V.get(), st.c, xtmp.get());
       DECO_CHECK_LAUNCH();
       if (!left) {
-        precond<double, double>(xtmp.get(), r);  // r used as scratch for z
-        axpy_into<double><<<g * 4, kThreads, 0, s>>>(n, r, x);
+        precond<double, double>(xtmp.get(), r);  // r is scratch for z here
+        axpy_into<double><<<nb, kThreads, 0, s>>>(n, r, x);
         DECO_CHECK_LAUNCH();
         spmv<double, double>(ctx, A, x, EpiResid<double, double>{b, r});
       } else {
-        axpy_into<double><<<g * 4, kThreads, 0, s>>>(n, xtmp.get(), x);
+        axpy_into<double><<<nb, kThreads, 0, s>>>(n, xtmp.get(), x);
         DECO_CHECK_LAUNCH();
         spmv<double, double>(ctx, A, x, EpiResid<double, double>{b, xtmp.get()});
         precond<double, double>(xtmp.get(), r);

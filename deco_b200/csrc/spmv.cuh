@@ -58,6 +58,10 @@ template <typename YT> struct EpiAdd {
   YT* y;
   __device__ void operator()(int o, double s) const { y[o] = (YT)((double)y[o] + s); }
 };
+template <typename YT> struct EpiStoreScaled {  // y = s * (A x), s read from device memory
+  YT* y; const double* s;
+  __device__ void operator()(int o, double v) const { y[o] = (YT)(__ldg(s) * v); }
+};
 template <typename ZT, typename YT> struct EpiResid {  // y = z - A x
   const ZT* z; YT* y;
   __device__ void operator()(int o, double s) const { y[o] = (YT)((double)z[o] - s); }

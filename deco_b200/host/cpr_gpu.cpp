@@ -124,12 +124,11 @@ int main(int argc, char** argv) {
     auto S = std::make_shared<SOL<int, int, double>>(param.get_child("sol"), A, P->apply, bp, nullptr, precision);
     sync();
     t_sol = now() - t_sol;
-    if (param.get<int>("sol.verbosity", 1) > 0) {
-      std::printf("\n--------------------------------\n");
-      std::printf("Profile of %s:\n", param.get<std::string>("sol.type") == "lgmres" ? "lGMRES" : "rGMRES");
-      std::printf("iteration count =  %d\n", S->iter);
-      std::printf("residual = %.2e\n", S->res_rel);
-    }
+    // the solver summary of rgmres.tpp:130-135 (printed here whatever sol.verbosity says)
+    std::printf("\n--------------------------------\n");
+    std::printf("Profile of %s:\n", param.get<std::string>("sol.type") == "lgmres" ? "lGMRES" : "rGMRES");
+    std::printf("iteration count =  %d\n", S->iter);
+    std::printf("residual = %.2e\n", S->res_rel);
     auto t = P->timings();
     std::printf("\nprofile (s)\n");
     std::printf("  setup & solve       %10.5f\n", t_prec + t_sol);
