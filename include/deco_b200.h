@@ -109,6 +109,16 @@ int deco_fsai_download(deco_ctx ctx, deco_fsai F, int* h_Lr, int* h_Lc, double* 
                        double* h_Uv);
 /* y = FU^T (FL x)  (FSAI::precond, FSAI.hpp:40-47).  d_x may equal d_y. */
 int deco_fsai_apply(deco_ctx ctx, deco_fsai F, const double* d_x, double* d_y);
+/* Same product as deco_fsai_apply, for callers that must not allocate device
+ * memory while they run (an application whose own pool owns all device memory
+ * after start-up, or a time-stepping loop that may not allocate once started).
+ * This call allocates nothing: the intermediate FL x lives in one fixed 8 MiB
+ * device array inside the library, shared by every call and every handle, so F
+ * may have at most 2^20 rows (larger factors return DECO_ERR_ARG).  The first
+ * call on a device looks up that array's address; make it before any stream
+ * capture.  Calls that overlap on the GPU (several streams at once) race on the
+ * array.  Has no counterpart in the reference. */
+int deco_fsai_apply_static(deco_ctx ctx, deco_fsai F, const double* d_x, double* d_y);
 
 /* -------------------------------------------------------------------- CPR
  * CPR<int,int,double,Mglobal,Mlocal>(const ptree& prec, shared_ptr<CSR> A, V*& b)
