@@ -67,9 +67,12 @@ class Context:
         check(lib().deco_ctx_set_autotune(self.h, int(on)))
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().deco_ctx_destroy(self.h)
-            self.h = None
+        try:
+            if getattr(self, "h", None):
+                lib().deco_ctx_destroy(self.h)
+                self.h = None
+        except Exception:  # interpreter shutdown: the binding may already be gone
+            pass
 
 
 _default = None
@@ -356,6 +359,7 @@ class SOL:
         self.iter, self.flag = res.iter, res.flag
         self.res_abs, self.res_rel = res.res_abs, res.res_rel
         self.time_ms, self.restarts = res.t_solve_ms, res.restarts
+        self.phases_ms = {"precond": res.t_precond_ms, "matvec": res.t_matvec_ms, "ortho": res.t_ortho_ms}
         self.resvec = self.resvec[: self.iter]
 
     def get_result(self):

@@ -75,21 +75,24 @@ class DevBuf {
   explicit DevBuf(size_t n, cudaStream_t s = 0) { alloc(n, s); }
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr; o.n_ = 0; }
+  DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_), s_(o.s_) { o.p_ = nullptr; o.n_ = 0; }
   DevBuf& operator=(DevBuf&& o) noexcept {
-    if (this != &o) { release(); p_ = o.p_; n_ = o.n_; o.p_ = nullptr; o.n_ = 0; }
+    if (this != &o) { release(); p_ = o.p_; n_ = o.n_; s_ = o.s_; o.p_ = nullptr; o.n_ = 0; }
     return *this;
   }
   ~DevBuf() { release(); }
 
+  // Stream-ordered allocation from the device's memory pool: no device-wide
+  // synchronisation, and freed blocks are reused by later allocations.
   void alloc(size_t n, cudaStream_t s = 0) {
     release();
     n_ = n;
+    s_ = s;
     void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, (n + kPad) * sizeof(T));
+    cudaError_t e = cudaMallocAsync(&p, (n + kPad) * sizeof(T), s);
     if (e != cudaSuccess) {
       cudaGetLastError();
-      throw Error(DECO_ERR_ALLOC, "cudaMalloc of " + std::to_string((n + kPad) * sizeof(T)) +
+      throw Error(DECO_ERR_ALLOC, "device allocation of " + std::to_string((n + kPad) * sizeof(T)) +
                                       " bytes failed: " + cudaGetErrorString(e));
     }
     p_ = static_cast<T*>(p);
@@ -99,7 +102,7 @@ class DevBuf {
     if (p_) DECO_CUDA(cudaMemsetAsync(p_, 0, (n_ + kPad) * sizeof(T), s));
   }
   void release() {
-    if (p_) cudaFree(p_);
+    if (p_) cudaFreeAsync(p_, s_);
     p_ = nullptr;
     n_ = 0;
   }
@@ -110,6 +113,7 @@ class DevBuf {
  private:
   T* p_ = nullptr;
   size_t n_ = 0;
+  cudaStream_t s_ = 0;
 };
 
 }  // namespace deco

@@ -1,6 +1,7 @@
 // context.cu — error state, context lifecycle and the device exclusive scan
 // used by every count/compact step (filters, pattern extraction, transposes).
 #include <atomic>
+#include <cstdlib>
 
 #include "common.cuh"
 
@@ -144,6 +145,14 @@ int deco_ctx_create(int device, void* stream, deco_ctx* out) {
     cudaDeviceProp prop;
     DECO_CUDA(cudaGetDeviceProperties(&prop, device));
     c->num_sms = prop.multiProcessorCount;
+    // DECO_AUTOTUNE=0 keeps the heuristic SpMV widths (profiler runs distort timings)
+    if (const char* e = std::getenv("DECO_AUTOTUNE")) c->autotune = std::atoi(e) != 0;
+    // keep freed device memory in the stream-ordered pool instead of returning it
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      unsigned long long threshold = ~0ULL;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    }
     DECO_CUDA(cudaEventCreate(&c->ev0));
     DECO_CUDA(cudaEventCreate(&c->ev1));
     DECO_CUDA(cudaMallocHost(&c->host_scalars, 1024 * sizeof(double)));

@@ -63,18 +63,16 @@ int tuned_subwarp(deco_ctx_s* ctx, deco_csr_s* A, bool f32) {
   cudaStreamCaptureStatus cs;
   DECO_CUDA(cudaStreamIsCapturing(ctx->stream, &cs));
   if (cs != cudaStreamCaptureStatusNone) return sw;
-  // time each candidate on a y = A x with x = ones (values only matter for timing)
+  // time the heuristic width and its neighbours on y = A x (x = 0: the values do
+  // not change the timing); keep the heuristic unless another width is clearly
+  // faster, so profiler-distorted timings cannot flip the choice at random
   DevBuf<double> x(A->m, ctx->stream), y(A->n, ctx->stream);
   DevBuf<float> xf, yf;
   x.zero(ctx->stream);
   if (f32) { xf.alloc(A->m, ctx->stream); yf.alloc(A->n, ctx->stream); xf.zero(ctx->stream); }
-  float best = 1e30f;
-  int best_sw = sw;
-  const int cands[] = {2, 4, 8, 16, 32};
-  for (int cand : cands) {
-    if (cand * W > 4 * (A->max_row + W) && cand > 2) continue;
-    float tot = 0.f;
-    for (int rep = 0; rep < 4; ++rep) {
+  auto time_width = [&](int cand) {
+    float t[5];
+    for (int rep = 0; rep < 6; ++rep) {
       DECO_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
       if (f32)
         launch_spmv_sw<float, float>(ctx->stream, cand, A->n, 1, A->r.get(), A->c.get(), A->v32.get(), xf.get(),
@@ -86,10 +84,21 @@ int tuned_subwarp(deco_ctx_s* ctx, deco_csr_s* A, bool f32) {
       DECO_CUDA(cudaEventSynchronize(ctx->ev1));
       float ms = 0.f;
       DECO_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-      if (rep > 0) tot += ms;  // first run warms caches
+      if (rep > 0) t[rep - 1] = ms;  // the first run warms caches
     }
-    if (tot < best) { best = tot; best_sw = cand; }
+    std::sort(t, t + 5);
+    return t[2];  // median
+  };
+  const int base = sw;
+  const float t_base = time_width(base);
+  float best = t_base;
+  int best_sw = base;
+  for (int cand : {base / 2, base * 2}) {
+    if (cand < 1 || cand > 32) continue;
+    const float tc = time_width(cand);
+    if (tc < best) { best = tc; best_sw = cand; }
   }
+  if (best > 0.95f * t_base) best_sw = base;
   sw = best_sw;
   std::lock_guard<std::mutex> lk(g_tuned_mu);
   g_tuned[key] = sw;

@@ -127,10 +127,20 @@ void box_smooth(std::vector<double>& f, int nx, int ny, int nz, bool vertical) {
 }
 
 void standardize(std::vector<double>& f, double sigma) {
+  // fixed chunks summed in order: the result does not depend on the thread count
+  const long long n = (long long)f.size();
+  const int nch = 1024;
+  std::vector<double> p1(nch, 0.0), p2(nch, 0.0);
+#pragma omp parallel for
+  for (int ch = 0; ch < nch; ++ch) {
+    const long long a = n * ch / nch, b = n * (ch + 1) / nch;
+    double t1 = 0, t2 = 0;
+    for (long long i = a; i < b; ++i) { t1 += f[i]; t2 += f[i] * f[i]; }
+    p1[ch] = t1;
+    p2[ch] = t2;
+  }
   double s1 = 0, s2 = 0;
-  long long n = (long long)f.size();
-#pragma omp parallel for reduction(+ : s1, s2)
-  for (long long i = 0; i < n; ++i) { s1 += f[i]; s2 += f[i] * f[i]; }
+  for (int ch = 0; ch < nch; ++ch) { s1 += p1[ch]; s2 += p2[ch]; }
   double mean = s1 / n, var = s2 / n - mean * mean, sd = var > 0 ? std::sqrt(var) : 1.0;
 #pragma omp parallel for
   for (long long i = 0; i < n; ++i) f[i] = (f[i] - mean) / sd * sigma;

@@ -24,6 +24,7 @@
 // rotations in float64; every restart recomputes the true residual b - A x and
 // the solution update in float64 (iterative refinement).
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "cpr.cuh"
@@ -111,46 +112,84 @@ __device__ void givens_apply(double c, double s, double& dx, double& dy) {
   dx = t;
 }
 
+// 128-bit vectors of the basis precision: 4 floats or 2 doubles per load
+template <typename T> struct Vec4;
+template <> struct Vec4<float> {
+  using t = float4;
+  static constexpr int N = 4;
+  __device__ static double dot(const float4& a, const float4& b) {
+    return (double)a.x * b.x + (double)a.y * b.y + (double)a.z * b.z + (double)a.w * b.w;
+  }
+  __device__ static float4 zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+  __device__ static double get(const float4& a, int e) { return e == 0 ? a.x : e == 1 ? a.y : e == 2 ? a.z : a.w; }
+};
+template <> struct Vec4<double> {
+  using t = double2;
+  static constexpr int N = 2;
+  __device__ static double dot(const double2& a, const double2& b) { return a.x * b.x + a.y * b.y; }
+  __device__ static double2 zero() { return make_double2(0.0, 0.0); }
+  __device__ static double get(const double2& a, int e) { return e == 0 ? a.x : a.y; }
+};
+
 // ---- pass A: raw dots u_c . w and u_c . u_j for c < ncols (u = stored columns).
-// Blocks own contiguous row ranges; warp w owns columns w, w+8, ...; lanes keep
-// per-column partial sums in registers for the whole range (no barriers).
+// Blocks own contiguous ranges of 128-bit vectors; warp w owns columns w, w+8, ...;
+// lanes keep per-column partial sums in registers for the whole range (no
+// barriers).  Rows past the last full vector are summed by the last block.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long ld, int ncols, int j,
                                                          const T* __restrict__ V, const T* __restrict__ w,
                                                          double* __restrict__ red, unsigned* counter, State st) {
+  using VT = typename Vec4<T>::t;
+  constexpr int N = Vec4<T>::N;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const T* __restrict__ uj = V + (size_t)j * ld;
-  const long long per = (n + gridDim.x - 1) / gridDim.x;
-  const long long r0 = per * blockIdx.x, r1 = min(n, r0 + per);
+  const long long nvec = n / N;
+  const long long per = (nvec + gridDim.x - 1) / gridDim.x;
+  const long long v0 = per * blockIdx.x, v1 = min(nvec, v0 + per);
+  const VT* __restrict__ wv4 = reinterpret_cast<const VT*>(w);
+  const VT* __restrict__ uv4 = reinterpret_cast<const VT*>(V + (size_t)j * ld);
   double pw[kColsPerWarp], pu[kColsPerWarp];
 #pragma unroll
   for (int k = 0; k < kColsPerWarp; ++k) { pw[k] = 0.0; pu[k] = 0.0; }
-  constexpr int step = 32 * kRowsPerLane;
-  for (long long base = r0; base < r1; base += step) {
-    double wv[kRowsPerLane], uv[kRowsPerLane];
+  constexpr int kVecPerLane = 4;
+  for (long long base = v0; base < v1; base += 32 * kVecPerLane) {
+    VT wv[kVecPerLane], uv[kVecPerLane];
 #pragma unroll
-    for (int q = 0; q < kRowsPerLane; ++q) {
-      const long long r = base + lane + 32 * q;
-      const bool ok = r < r1;
-      wv[q] = ok ? (double)w[r] : 0.0;
-      uv[q] = ok ? (double)uj[r] : 0.0;
+    for (int q = 0; q < kVecPerLane; ++q) {
+      const long long vi = base + lane + 32 * q;
+      wv[q] = vi < v1 ? wv4[vi] : Vec4<T>::zero();
+      uv[q] = vi < v1 ? uv4[vi] : Vec4<T>::zero();
     }
 #pragma unroll
     for (int k = 0; k < kColsPerWarp; ++k) {
       const int c = warp + k * kWarps;
       if (c < ncols) {
-        const T* __restrict__ vc = V + (size_t)c * ld;
+        const VT* __restrict__ vc = reinterpret_cast<const VT*>(V + (size_t)c * ld);
+        VT v[kVecPerLane];
 #pragma unroll
-        for (int q = 0; q < kRowsPerLane; ++q) {
-          const long long r = base + lane + 32 * q;
-          if (r < r1) {
-            const double v = ldv(vc + r);
-            pw[k] += v * wv[q];
-            pu[k] += v * uv[q];
-          }
+        for (int q = 0; q < kVecPerLane; ++q) {
+          const long long vi = base + lane + 32 * q;
+          v[q] = vi < v1 ? __ldcs(vc + vi) : Vec4<T>::zero();
+        }
+#pragma unroll
+        for (int q = 0; q < kVecPerLane; ++q) {
+          pw[k] += Vec4<T>::dot(v[q], wv[q]);
+          pu[k] += Vec4<T>::dot(v[q], uv[q]);
         }
       }
     }
+  }
+  if (blockIdx.x == gridDim.x - 1 && lane == 0) {  // rows past the last full vector
+    const T* __restrict__ uj = V + (size_t)j * ld;
+    for (long long r = nvec * N; r < n; ++r)
+#pragma unroll
+      for (int k = 0; k < kColsPerWarp; ++k) {
+        const int c = warp + k * kWarps;
+        if (c < ncols) {
+          const double v = (double)V[(size_t)c * ld + r];
+          pw[k] += v * (double)w[r];
+          pu[k] += v * (double)uj[r];
+        }
+      }
   }
 #pragma unroll
   for (int k = 0; k < kColsPerWarp; ++k) {
@@ -184,23 +223,53 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long 
   }
 }
 
-// ---- pass B: w'' = w - sum_c coef_c u_c, stored as column j+1; ||w''||^2
+// ---- pass B: w'' = w - sum_c coef_c u_c, stored as column j+1; ||w''||^2.
+// One thread per 128-bit vector of rows; the column loop is unrolled so several
+// independent vector loads are in flight per thread.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) arnoldi_update(long long n, long long ld, int ncols, int j,
                                                            const T* __restrict__ V, const T* __restrict__ w,
                                                            T* __restrict__ out, double* __restrict__ red,
                                                            unsigned* counter, State st) {
+  using VT = typename Vec4<T>::t;
+  constexpr int N = Vec4<T>::N;
   __shared__ double cs_[kMaxCols];
   for (int i = threadIdx.x; i < ncols; i += kThreads) cs_[i] = st.c[i];
   __syncthreads();
+  const long long nvec = n / N;
   double ss = 0.0;
-  for (long long r = (long long)blockIdx.x * kThreads + threadIdx.x; r < n; r += (long long)gridDim.x * kThreads) {
-    double x = (double)w[r];
-#pragma unroll 8
-    for (int i = 0; i < ncols; ++i) x -= cs_[i] * ldv(V + (size_t)i * ld + r);
-    const T xq = (T)x;
-    out[r] = xq;
-    ss += (double)xq * (double)xq;
+  for (long long vi = (long long)blockIdx.x * kThreads + threadIdx.x; vi < nvec;
+       vi += (long long)gridDim.x * kThreads) {
+    const VT wv = reinterpret_cast<const VT*>(w)[vi];
+    double x[N];
+#pragma unroll
+    for (int e = 0; e < N; ++e) x[e] = Vec4<T>::get(wv, e);
+#pragma unroll 4
+    for (int i = 0; i < ncols; ++i) {
+      const VT v = __ldcs(reinterpret_cast<const VT*>(V + (size_t)i * ld) + vi);
+      const double ci = cs_[i];
+#pragma unroll
+      for (int e = 0; e < N; ++e) x[e] -= ci * Vec4<T>::get(v, e);
+    }
+    T o[N];
+#pragma unroll
+    for (int e = 0; e < N; ++e) {
+      o[e] = (T)x[e];
+      ss += (double)o[e] * (double)o[e];
+    }
+    VT ov;
+    if constexpr (N == 4) ov = make_float4(o[0], o[1], o[2], o[3]);
+    else ov = make_double2(o[0], o[1]);
+    reinterpret_cast<VT*>(out)[vi] = ov;
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {  // rows past the last full vector
+    for (long long r = nvec * N; r < n; ++r) {
+      double x = (double)w[r];
+      for (int i = 0; i < ncols; ++i) x -= cs_[i] * (double)V[(size_t)i * ld + r];
+      const T xq = (T)x;
+      out[r] = xq;
+      ss += (double)xq * (double)xq;
+    }
   }
   block_sum_to(ss, red + blockIdx.x);
   if (!last_block(counter)) return;
@@ -311,6 +380,13 @@ struct Solver {
   DevBuf<T> V, w, z;
   DevBuf<double> st_buf, xtmp, r64, norm;
   State st{};
+  // DECO_PROFILE=1: events around the phases of every Arnoldi step of a cycle
+  bool profile = false;
+  std::vector<cudaEvent_t> pev;
+  double t_phase[3] = {0, 0, 0};
+  ~Solver() {
+    for (auto e : pev) cudaEventDestroy(e);
+  }
 
   Solver(deco_ctx_s* c, deco_csr_s* a, deco_cpr_s* p, const deco_sol_params& pr) : ctx(c), A(a), P(p), prm(pr) {
     n = A->n;
@@ -328,6 +404,25 @@ struct Solver {
     norm.alloc(4, s);
     const size_t need = (size_t)(2 * (m + 2)) * nb;
     if (ctx->red.size() < need) ctx->red.alloc(need, s);
+    if (const char* e = std::getenv("DECO_PROFILE")) profile = std::atoi(e) != 0;
+    if (profile) {
+      pev.resize(4 * (size_t)(m + 1));
+      for (auto& e : pev) DECO_CUDA(cudaEventCreate(&e));
+    }
+  }
+
+  // adds the phase times of steps [0, steps) of the cycle that just finished
+  void collect(int steps) {
+    if (!profile) return;
+    for (int j = 0; j < steps; ++j) {
+      float a = 0, b = 0, c = 0;
+      DECO_CUDA(cudaEventElapsedTime(&a, pev[4 * j], pev[4 * j + 1]));
+      DECO_CUDA(cudaEventElapsedTime(&b, pev[4 * j + 1], pev[4 * j + 2]));
+      DECO_CUDA(cudaEventElapsedTime(&c, pev[4 * j + 2], pev[4 * j + 3]));
+      t_phase[0] += a;
+      t_phase[1] += b;
+      t_phase[2] += c;
+    }
   }
 
   T* col(int i) { return V.get() + (size_t)i * ld; }
@@ -372,19 +467,26 @@ struct Solver {
   void arnoldi_step(int j, bool left, volatile double* hsc, cudaEvent_t* ev) {
     cudaStream_t s = ctx->stream;
     const double* sj = st.s + j;
+    // phase order per step: [pev0] precond [pev1] matvec [pev2] ortho [pev3]
+    // (left GMRES runs the matvec first; its phases are recorded accordingly)
+    if (profile) DECO_CUDA(cudaEventRecord(pev[4 * j], s));
     if (!left) {
       precond<T, T>(col(j), z.get());
+      if (profile) DECO_CUDA(cudaEventRecord(pev[4 * j + 1], s));
       matvec_scaled<T>(z.get(), w.get(), sj);
     } else {
       matvec_scaled<T>(col(j), z.get(), sj);
+      if (profile) DECO_CUDA(cudaEventRecord(pev[4 * j + 1], s));
       precond<T, T>(z.get(), w.get());
     }
+    if (profile) DECO_CUDA(cudaEventRecord(pev[4 * j + 2], s));
     const int nc = j + 1;
     arnoldi_dots<T><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V.get(), w.get(), ctx->red.get(), ctx->counter.get(), st);
     DECO_CHECK_LAUNCH();
     arnoldi_update<T><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V.get(), w.get(), col(j + 1), ctx->red.get(),
                                               ctx->counter.get(), st);
     DECO_CHECK_LAUNCH();
+    if (profile) DECO_CUDA(cudaEventRecord(pev[4 * j + 3], s));
     DECO_CUDA(cudaMemcpyAsync(const_cast<double*>(hsc) + (j & 1), st.sc + SC_RES, sizeof(double),
                               cudaMemcpyDeviceToHost, s));
     DECO_CUDA(cudaEventRecord(ev[j & 1], s));
@@ -424,7 +526,7 @@ struct Solver {
       DECO_CUDA(cudaStreamSynchronize(s));
       double gj = hsc[2];
       bool known = true;  // |g_j| is on the host; otherwise it is in flight from step j-1
-      int j = 0;
+      int j = 0, launched = 0;
       for (;;) {
         // the reference's loop bounds and inner convergence check (rgmres.tpp:58-66)
         if (!(j < m && iter < itmax)) break;
@@ -433,12 +535,14 @@ struct Solver {
           if (resvec) resvec[iter] = rnorm / bnorm;
           if (rnorm < abstol) { flag = 0; break; }
           arnoldi_step(j, left, hsc, ev);
+          launched = j + 1;
         } else {
           // enqueue step j before looking at |g_j| from step j-1; if |g_j| already
           // meets the tolerance, step j is dropped: it wrote only column j of H/G,
           // g_{j+1}, rotation j and basis column j+1, which the back substitution
           // over j columns never reads
           arnoldi_step(j, left, hsc, ev);
+          launched = j + 1;
           DECO_CUDA(cudaEventSynchronize(ev[(j - 1) & 1]));
           gj = hsc[(j - 1) & 1];
           rnorm = fabs(gj);
@@ -455,6 +559,7 @@ struct Solver {
       DECO_CUDA(cudaStreamSynchronize(s));
       if (hsc[3] != 0.0)
         throw Error(DECO_ERR_BREAKDOWN, "Error in rgmres: Zero diagonal element in upper triangular matrix.");
+      collect(launched);
       combine<T, double><<<nb, kThreads, 0, s>>>(n, ld, j > 0 ? j : 1, V.get(), st.c, xtmp.get());
       DECO_CHECK_LAUNCH();
       if (!left) {
@@ -482,6 +587,9 @@ struct Solver {
     res->res_rel = rnorm / bnorm;
     res->t_solve_ms = ms;
     res->restarts = restarts;
+    res->t_precond_ms = t_phase[0];
+    res->t_matvec_ms = t_phase[1];
+    res->t_ortho_ms = t_phase[2];
     if (prm.verbosity > 0) {
       std::printf("\n--------------------------------\n");
       std::printf("Profile of %s:\n", left ? "lGMRES" : "rGMRES");

@@ -126,11 +126,12 @@ void launch_spmv_sw(cudaStream_t st, int sw, int nrows_out, int row_stride, cons
   DECO_CHECK_LAUNCH();
 }
 
-// heuristic width: enough lanes that one pass of vector loads covers the row
+// heuristic width: about two vector loads per lane per row, the best width
+// measured on B200 for 7- and 14-entry rows in float64 (W = 2) and float32 (W = 4)
 inline int heuristic_subwarp(double avg_row, int W) {
-  double loads = avg_row / W + 1.0;
+  const double half_loads = avg_row / (2.0 * W);
   int sw = 1;
-  while (sw < 32 && sw < loads) sw <<= 1;
+  while (sw < 32 && sw < half_loads) sw <<= 1;
   return sw;
 }
 

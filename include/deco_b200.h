@@ -183,6 +183,10 @@ typedef struct deco_sol_result {
   double res_rel;        /* res_abs / ||b|| (SOL::res_rel)                   */
   double t_solve_ms;     /* device time of the solve                         */
   int restarts;          /* completed restart cycles                         */
+  /* with the environment variable DECO_PROFILE=1: device time summed over the
+   * Arnoldi steps spent in the preconditioner, in the SpMV with A, and in the
+   * orthogonalisation (0 otherwise) */
+  double t_precond_ms, t_matvec_ms, t_ortho_ms;
 } deco_sol_result;
 
 /* Solves A x = b with preconditioner P (NULL: identity).  A and d_b are the

@@ -72,3 +72,21 @@ def test_invalid_parameters_are_rejected():
     p.bs = 4
     with pytest.raises(ValueError):
         gen.generate(p)
+
+
+def test_independent_of_thread_count():
+    """Every draw is a counter-based hash and every reduction sums fixed chunks in
+    order, so the system is the same for any OpenMP thread count."""
+    import hashlib
+    import os
+    import subprocess
+    import sys
+    code = ("import sys, hashlib; sys.path.insert(0, %r); from deco_b200 import gen; "
+            "s = gen.generate(gen.preset(5)); print(hashlib.md5(s.v.tobytes() + s.b.tobytes()).hexdigest())"
+            % os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    digests = set()
+    for t in ("1", "3", "8"):
+        env = dict(os.environ, OMP_NUM_THREADS=t)
+        out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, check=True)
+        digests.add(out.stdout.strip())
+    assert len(digests) == 1
