@@ -299,27 +299,45 @@ def main():
     Fg = P64.fsai(0)
     nzF = Fg.nz
     kernels = {}
+
+    def matrix_bytes(nz, blocks, vb):
+        """Bytes of one pass over a matrix in the layout the product reads: the
+        cell-block copy (one 4-byte index per bs x bs block, block-row pointers)
+        when there is one, else CSR (4-byte index + value per entry)."""
+        bsz, nblk = blocks
+        if bsz:
+            return nblk * 4 + nblk * bsz * bsz * vb + 4 * (n // bsz + 1)
+        return nz * (4 + vb) + 4 * (n + 1)
+
+    fmt = "cell-block (bs %d)" % A.blocks[0] if A.blocks[0] else "CSR"
     ms = kernel_ms(lambda: A.apply_f32(x32, y32))
-    alg32 = 8 * nnz + 4 * (n + 1) + 4 * n + 4 * n
-    kernels["spmv_A_f32"] = {"ms": ms, "gbs": alg32 / ms / 1e6, "alg_bytes": alg32, "subwarp": A.subwarp}
+    alg32 = matrix_bytes(nnz, A.blocks, 4) + 4 * n + 4 * n
+    kernels["spmv_A_f32"] = {"ms": ms, "gbs": alg32 / ms / 1e6, "alg_bytes": alg32, "format": fmt,
+                             "subwarp": A.subwarp}
     ms = kernel_ms(lambda: A.apply(x64, y64))
-    alg64 = 12 * nnz + 4 * (n + 1) + 8 * n + 8 * n
-    kernels["spmv_A_f64"] = {"ms": ms, "gbs": alg64 / ms / 1e6, "alg_bytes": alg64}
+    alg64 = matrix_bytes(nnz, A.blocks, 8) + 8 * n + 8 * n
+    kernels["spmv_A_f64"] = {"ms": ms, "gbs": alg64 / ms / 1e6, "alg_bytes": alg64, "format": fmt}
+    fb, kl, ku = Fg.blocks
     ms = kernel_ms(lambda: Fg.apply(x64, y64))
-    algF = 2 * (12 * nzF + 4 * (n + 1)) + 8 * n + 2 * 8 * n + 8 * n
-    kernels["fsai_apply_global_f64"] = {"ms": ms, "gbs": algF / ms / 1e6, "alg_bytes": algF, "nnz_factor": nzF}
+    algF = matrix_bytes(nzF, (fb, kl), 8) + matrix_bytes(nzF, (fb, ku), 8) + 8 * n + 2 * 8 * n + 8 * n
+    kernels["fsai_apply_global_f64"] = {"ms": ms, "gbs": algF / ms / 1e6, "alg_bytes": algF, "nnz_factor": nzF,
+                                        "format": "cell-block (bs %d)" % fb if fb else "CSR"}
     del P64
     P32 = d.CPR(PREC, d.CSR(n, n, r_d, c_d, v_d, ctx), b_d.clone(), precision=32)
     Fg32 = P32.fsai(0)
+    fb, kl, ku = Fg32.blocks
     ms = kernel_ms(lambda: Fg32.apply(x64, y64))
-    algF32 = 2 * (8 * nzF + 4 * (n + 1)) + 8 * n + 2 * 4 * n + 8 * n
-    kernels["fsai_apply_global_f32"] = {"ms": ms, "gbs": algF32 / ms / 1e6, "alg_bytes": algF32}
+    algF32 = matrix_bytes(nzF, (fb, kl), 4) + matrix_bytes(nzF, (fb, ku), 4) + 8 * n + 2 * 4 * n + 8 * n
+    kernels["fsai_apply_global_f32"] = {"ms": ms, "gbs": algF32 / ms / 1e6, "alg_bytes": algF32,
+                                        "format": "cell-block (bs %d)" % fb if fb else "CSR"}
     del P32
     for k in kernels.values():
         k["frac_of_peak"] = k["gbs"] / peak
     dom = kernels["spmv_A_f32"]
     roofline = {"bound": "hbm", "achieved": dom["gbs"], "peak": peak, "unit": "GB/s", "frac": dom["gbs"] / peak,
-                "traffic": None, "kernel": "deco::spmv_kernel<float> on A (8M rows, 111.36M nnz, float32 values)",
+                "traffic": None,
+                "kernel": ("deco::bsr_kernel<float> (cell blocks)" if A.blocks[0] else "deco::spmv_kernel<float> (CSR)")
+                + " on A (8M rows, 111.36M nnz, float32 values)",
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind}
 
     cpu = None

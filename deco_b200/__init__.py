@@ -8,6 +8,8 @@ tensors; the native library does all the work.
   FSAI  precond/FSAI/FSAI.hpp   FSAI(param, A); apply(x, b) (x may be b)
   CPR   precond/CPR.hpp         CPR(prec, A, b) mutates A and b; apply(r, x)
   SOL   solver/SOL.hpp          SOL(sol, A, precond, b, x=None) solves in the constructor
+  ADJ   (no reference counterpart) adjoint of the solve: A^T lambda = g with CPR on A^T;
+        deco_b200.adjoint wraps forward + adjoint as a torch.autograd.Function
 
 Parameter dictionaries use the reference's JSON keys (values may be strings, as
 in the shipped param_*.json files).
@@ -21,7 +23,7 @@ import numpy as np
 
 from ._lib import CprParams, DecoError, SolParams, SolResult, check, lib
 
-__all__ = ["Context", "CSR", "FSAI", "CPR", "SOL", "DecoError", "default_context", "load_params",
+__all__ = ["Context", "CSR", "FSAI", "CPR", "SOL", "ADJ", "DecoError", "default_context", "load_params",
            "cpr_params", "sol_params"]
 
 _WEIGHTS = {"none": 0, "quasiimpes": 1, "quasiimpes_GE": 2}
@@ -168,8 +170,42 @@ class CSR:
         return r, c, v
 
     def set_values(self, v):
+        if hasattr(v, "data_ptr"):
+            torch = _torch()
+            assert v.dtype == torch.float64 and v.is_contiguous() and v.numel() == self.nz
+            check(lib().deco_csr_set_values(self.ctx.h, self.h, _ptr(v), 1 if v.is_cuda else 0))
+            return
         v = np.ascontiguousarray(v, np.float64)
         check(lib().deco_csr_set_values(self.ctx.h, self.h, v.ctypes.data, 0))
+
+    def set_blocks(self, bs: int):
+        """Adds (bs 2 or 3) or removes (0) the cell-block copy used by later products."""
+        check(lib().deco_csr_set_blocks(self.ctx.h, self.h, int(bs)))
+
+    @property
+    def blocks(self):
+        """(block size, stored blocks) of the cell-block copy; (0, 0) without one."""
+        b, k = C.c_int(), C.c_int()
+        check(lib().deco_csr_blocks(self.h, C.byref(b), C.byref(k)))
+        return b.value, k.value
+
+    def transpose(self) -> "CSR":
+        """A^T on the device, rows in ascending column order."""
+        h = C.c_void_p()
+        check(lib().deco_csr_transpose(self.ctx.h, self.h, C.byref(h)))
+        T = CSR(0, 0, None, None, None, ctx=self.ctx, _handle=h)
+        T._borrowed = False
+        return T
+
+    def grad_pattern(self, lam, x, alpha: float = -1.0, out=None):
+        """out[e] = alpha * lam[i] * x[j] for every stored entry e = (i, j): dL/dA for alpha = -1."""
+        torch = _torch()
+        lam = _dev(lam, torch.float64)
+        x = _dev(x, torch.float64)
+        if out is None:
+            out = torch.empty(self.nz, dtype=torch.float64, device="cuda")
+        check(lib().deco_grad_A_pattern(self.ctx.h, self.h, _ptr(lam), _ptr(x), float(alpha), _ptr(out)))
+        return out
 
     @property
     def subwarp(self) -> int:
@@ -215,6 +251,13 @@ class FSAI:
             b = torch.empty(self.n, dtype=torch.float64, device="cuda")
         check(lib().deco_fsai_apply(self.ctx.h, self.h, _ptr(x), _ptr(b)))
         return b
+
+    @property
+    def blocks(self):
+        """(block size, stored blocks of FL, stored blocks of FU^T); block size 0 without block copies."""
+        b, kl, ku = C.c_int(), C.c_int(), C.c_int()
+        check(lib().deco_fsai_blocks(self.h, C.byref(b), C.byref(kl), C.byref(ku)))
+        return b.value, kl.value, ku.value
 
     def factors(self):
         n, nz = self.n, self.nz
@@ -280,7 +323,17 @@ def cpr_params(prec: dict, precision: int = 64) -> CprParams:
         tol_zero=float(prec.get("tol_zero", 0.0)), glo_tol_rel=float(g.get("tol_rel", 0.0)),
         glo_tol_abs=float(g.get("tol_abs", 0.0)), glo_power=int(g.get("power", 1)),
         loc_tol_rel=float(l.get("tol_rel", 0.0)), loc_tol_abs=float(l.get("tol_abs", 0.0)),
-        loc_power=int(l.get("power", 1)), precision=int(precision))
+        loc_power=int(l.get("power", 1)), precision=int(precision), glo_type=_stage(g.get("type", "FSAI")),
+        loc_type=_stage(l.get("type", "FSAI")), glo_block_size=int(g.get("block_size", prec["block_size"])),
+        loc_block_size=int(l.get("block_size", 1)))
+
+
+def _stage(t: str) -> int:
+    if t == "FSAI":
+        return 0
+    if t == "Jacobi":
+        return 1
+    raise DecoError(-6, f"the GPU path builds FSAI or Jacobi stages (got {t}); hypre AMG stays on the CPU build")
 
 
 def sol_params(sol: dict, precision: int = 64, use_x0: bool = False) -> SolParams:
@@ -307,10 +360,16 @@ class CPR:
         check(lib().deco_cpr_create(self.ctx.h, A.h, _ptr(b), C.byref(self.params), C.byref(h)))
         self.h = h
         self.n = A.n
+
+    @property
+    def Ap(self) -> CSR:
+        """The pressure matrix A_pp (borrowed: the returned object keeps this CPR alive;
+        the CPR holds no reference back, so dropping the CPR frees its device memory at once)."""
         hp = C.c_void_p()
         check(lib().deco_cpr_pressure(self.h, C.byref(hp)))
-        self.Ap = CSR(0, 0, None, None, None, ctx=self.ctx, _handle=hp)
-        self.Ap._owner = self
+        M = CSR(0, 0, None, None, None, ctx=self.ctx, _handle=hp)
+        M._owner = self
+        return M
 
     def fsai(self, which: int) -> FSAI:
         hf = C.c_void_p()
@@ -324,6 +383,14 @@ class CPR:
             x = torch.empty(self.n, dtype=torch.float64, device="cuda")
         check(lib().deco_cpr_apply(self.ctx.h, self.h, _ptr(r), _ptr(x)))
         return x
+
+    def decouple_rhs(self, b):
+        """Decouples another right-hand side in place, bit-identically to the b given at setup."""
+        torch = _torch()
+        if not (hasattr(b, "is_cuda") and b.is_cuda and b.dtype == torch.float64 and b.is_contiguous()):
+            raise DecoError(-1, "b must be a contiguous CUDA float64 tensor (it is decoupled in place)")
+        check(lib().deco_cpr_decouple_rhs(self.ctx.h, self.h, _ptr(b)))
+        return b
 
     def timings(self) -> dict:
         t = (C.c_double * 5)()
@@ -364,3 +431,50 @@ class SOL:
 
     def get_result(self):
         return self.x
+
+
+class ADJ:
+    """Adjoint of the CPR-GMRES solve (no counterpart in the reference).
+
+    ``ADJ(prec, A)`` transposes A (its current values: build it before any forward
+    decoupling) and sets up CPR on A^T; ``solve(sol, g)`` returns lambda with
+    A^T lambda = g.  dL/db = lambda; dL/dA on A's pattern is
+    ``A.grad_pattern(lambda, x)``."""
+
+    def __init__(self, prec: dict, A: CSR, precision: int = 64):
+        self.ctx = A.ctx
+        self.n = A.n
+        self.params = cpr_params(prec, precision)
+        h = C.c_void_p()
+        check(lib().deco_adjoint_create(self.ctx.h, A.h, C.byref(self.params), C.byref(h)))
+        self.h = h
+
+    def solve(self, sol: dict, g, lam=None, precision: int | None = None):
+        torch = _torch()
+        prec = self.params.precision if precision is None else precision
+        sp = sol_params(sol, prec, use_x0=lam is not None)
+        g = _dev(g, torch.float64)
+        if lam is None:
+            lam = torch.zeros(self.n, dtype=torch.float64, device="cuda")
+        res = SolResult()
+        self.resvec = np.zeros(max(sp.itmax, 0) + 1)
+        check(lib().deco_adjoint_solve(self.ctx.h, self.h, _ptr(g), _ptr(lam), C.byref(sp), C.byref(res),
+                                       self.resvec.ctypes.data))
+        self.iter, self.flag = res.iter, res.flag
+        self.res_abs, self.res_rel = res.res_abs, res.res_rel
+        self.time_ms = res.t_solve_ms
+        self.resvec = self.resvec[: self.iter]
+        return lam
+
+    def transposed(self) -> CSR:
+        """A^T as decoupled by the adjoint's CPR (owned by this object)."""
+        h = C.c_void_p()
+        check(lib().deco_adjoint_parts(self.h, C.byref(h), None))
+        T = CSR(0, 0, None, None, None, ctx=self.ctx, _handle=h)
+        T._owner = self
+        return T
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().deco_adjoint_destroy(self.h)
+            self.h = None

@@ -22,7 +22,8 @@ class CprParams(C.Structure):
                 ("use_drs", C.c_int), ("drs_e_dd", C.c_double), ("drs_e_ps", C.c_double), ("cpd", C.c_int),
                 ("tol_zero", C.c_double), ("glo_tol_rel", C.c_double), ("glo_tol_abs", C.c_double),
                 ("glo_power", C.c_int), ("loc_tol_rel", C.c_double), ("loc_tol_abs", C.c_double),
-                ("loc_power", C.c_int), ("precision", C.c_int)]
+                ("loc_power", C.c_int), ("precision", C.c_int), ("glo_type", C.c_int), ("loc_type", C.c_int),
+                ("glo_block_size", C.c_int), ("loc_block_size", C.c_int)]
 
 
 class SolParams(C.Structure):
@@ -54,12 +55,15 @@ SIGNATURES = {
     "deco_csr_make_f32": ([vp, vp], C.c_int),
     "deco_csr_subwarp": ([vp, ip], C.c_int),
     "deco_csr_set_subwarp": ([vp, C.c_int], C.c_int),
+    "deco_csr_set_blocks": ([vp, vp, C.c_int], C.c_int),
+    "deco_csr_blocks": ([vp, ip, ip], C.c_int),
     "deco_spmv": ([vp, vp, vp, vp, C.c_int], C.c_int),
     "deco_spmv_f32": ([vp, vp, vp, vp, C.c_int], C.c_int),
     "deco_residual": ([vp, vp, vp, vp, vp], C.c_int),
     "deco_fsai_create": ([vp, vp, C.c_double, C.c_double, C.c_int, C.c_int, C.POINTER(vp)], C.c_int),
     "deco_fsai_destroy": ([vp], C.c_int),
     "deco_fsai_info": ([vp, ip, ip, ip], C.c_int),
+    "deco_fsai_blocks": ([vp, ip, ip, ip], C.c_int),
     "deco_fsai_download": ([vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
     "deco_fsai_apply": ([vp, vp, vp, vp], C.c_int),
     "deco_fsai_apply_static": ([vp, vp, vp, vp], C.c_int),
@@ -70,7 +74,14 @@ SIGNATURES = {
     "deco_cpr_fsai": ([vp, C.c_int, C.POINTER(vp)], C.c_int),
     "deco_cpr_timings": ([vp, dp], C.c_int),
     "deco_cpr_fixed_diagonals": ([vp, ip], C.c_int),
+    "deco_cpr_decouple_rhs": ([vp, vp, vp], C.c_int),
     "deco_gmres_solve": ([vp, vp, vp, vp, vp, C.POINTER(SolParams), C.POINTER(SolResult), vp], C.c_int),
+    "deco_csr_transpose": ([vp, vp, C.POINTER(vp)], C.c_int),
+    "deco_grad_A_pattern": ([vp, vp, vp, vp, C.c_double, vp], C.c_int),
+    "deco_adjoint_create": ([vp, vp, C.POINTER(CprParams), C.POINTER(vp)], C.c_int),
+    "deco_adjoint_destroy": ([vp], C.c_int),
+    "deco_adjoint_solve": ([vp, vp, vp, vp, C.POINTER(SolParams), C.POINTER(SolResult), vp], C.c_int),
+    "deco_adjoint_parts": ([vp, C.POINTER(vp), C.POINTER(vp)], C.c_int),
 }
 
 _lib = None

@@ -126,6 +126,7 @@ struct deco_ctx_s {
   bool own_stream = false;
   int num_sms = 148;
   int autotune = 1;
+  int bsr = 1;        // cell-block copies for CPR systems (DECO_BSR=0 disables)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // small pinned host buffer for scalar read-backs
   double* host_scalars = nullptr;

@@ -147,6 +147,7 @@ int deco_ctx_create(int device, void* stream, deco_ctx* out) {
     c->num_sms = prop.multiProcessorCount;
     // DECO_AUTOTUNE=0 keeps the heuristic SpMV widths (profiler runs distort timings)
     if (const char* e = std::getenv("DECO_AUTOTUNE")) c->autotune = std::atoi(e) != 0;
+    if (const char* e = std::getenv("DECO_BSR")) c->bsr = std::atoi(e) != 0;
     // keep freed device memory in the stream-ordered pool instead of returning it
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {

@@ -46,6 +46,8 @@ struct DecoupleArgs {
   double* v;
   double* b;
   double* w;
+  double* w0;              // quasi-IMPES weights as computed (before the DRS reset)
+  unsigned char* ops;      // per cell: bits 0-2 rows kept by DRS, bit 3 rows 1 and 2 swapped
   double* J;
   char* chk;
   int* err;
@@ -99,6 +101,7 @@ __global__ void cpr_decouple(DecoupleArgs a) {
 
     // ---- fix_diag (CPR.hpp:753-840), small_tol = big_tol = 1e-20
     const double tol = 1e-20;
+    unsigned char op = 0;
     {
       int j0 = bsearch_le(c, r[i0], r[i0 + 1], i0);
       if (fabs(v[j0]) < tol) { v[j0] = (v[j0] > 0) ? tol : -tol; a.chk[i0] = 1; atomicAdd(a.nfixed, 1); }
@@ -110,6 +113,7 @@ __global__ void cpr_decouple(DecoupleArgs a) {
             const int ia1 = r[i0 + 1], ib1 = r[i0 + 2];
             for (int t = 0; t < ib1 - ia1; ++t) { double x = v[ia1 + t]; v[ia1 + t] = v[ib1 + t]; v[ib1 + t] = x; }
             double x = b[i0 + 1]; b[i0 + 1] = b[i0 + 2]; b[i0 + 2] = x;
+            op |= 8;
           } else {
             if (fabs(v[j1]) < tol) { v[j1] = (v[j1] > 0) ? tol : -tol; a.chk[i0 + 1] = 1; atomicAdd(a.nfixed, 1); }
             if (fabs(v[j2]) < tol) { v[j2] = (v[j2] > 0) ? tol : -tol; a.chk[i0 + 2] = 1; atomicAdd(a.nfixed, 1); }
@@ -164,6 +168,7 @@ __global__ void cpr_decouple(DecoupleArgs a) {
       w[a.pid] = 1.0;
       small_lu_solve(bs, B, w);
     }
+    for (int p = 0; p < bs; ++p) a.w0[i0 + p] = w[p];
     if (a.weights != 0) {
       for (int p = 0; p < bs; ++p) {
         const int i = i0 + p;
@@ -206,6 +211,8 @@ __global__ void cpr_decouple(DecoupleArgs a) {
           }
     }
     for (int p = 0; p < bs; ++p) a.w[i0 + p] = w[p];
+    for (int p = 0; p < bs; ++p) op |= wd[p] ? (1 << p) : 0;
+    a.ops[s] = op;
 
     // ---- IMPES (CPR.hpp:450-516): pressure row (offset 0) accumulates the others
     {
@@ -289,6 +296,41 @@ __global__ void cpr_decouple(DecoupleArgs a) {
   }
 }
 
+// The right-hand-side half of cpr_decouple for a new vector: the same row
+// operations of every cell (row swap, weights, DRS undo, IMPES sum, CPD), with
+// the same separately rounded arithmetic in the same order, so a vector
+// replayed here is bit-identical to one decoupled together with A.
+__global__ void cpr_decouple_rhs(int sn, int bs, int weights, int use_drs, int cpd, const double* __restrict__ w0,
+                                 const unsigned char* __restrict__ ops, const double* __restrict__ J,
+                                 double* __restrict__ b) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < sn; s += gridDim.x * blockDim.x) {
+    const long long i0 = (long long)s * bs;
+    const unsigned op = ops[s];
+    double x[3];
+    for (int p = 0; p < bs; ++p) x[p] = b[i0 + p];
+    if (op & 8) { double t = x[1]; x[1] = x[2]; x[2] = t; }
+    if (weights != 0) {
+      for (int p = 0; p < bs; ++p) x[p] = dmul(x[p], w0[i0 + p]);
+      if (use_drs)
+        for (int p = 0; p < bs; ++p)
+          if (!(op & (1u << p))) x[p] = ddiv(x[p], w0[i0 + p]);
+    }
+    double sum = 0.0;
+    for (int j = 0; j < bs; ++j) sum = madd(sum, use_drs ? ((op & (1u << j)) ? 1.0 : 0.0) : 1.0, x[j]);
+    x[0] = sum;
+    if (cpd) {
+      const double* o = J + (long long)s * bs * bs;
+      double y[3];
+      for (int p = 0; p < bs; ++p) {
+        y[p] = 0.0;
+        for (int j = 0; j < bs; ++j) y[p] = madd(y[p], o[p * bs + j], x[j]);
+      }
+      for (int p = 0; p < bs; ++p) x[p] = y[p];
+    }
+    for (int p = 0; p < bs; ++p) b[i0 + p] = x[p];
+  }
+}
+
 __global__ void unfix_diag(int n, const int* __restrict__ r, const int* __restrict__ c, double* __restrict__ v,
                            const char* __restrict__ chk) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -361,8 +403,9 @@ static void cpr_build(deco_ctx_s* ctx, deco_csr_s* A, double* d_b, const deco_cp
   DECO_REQUIRE(A->n % bs == 0, DECO_ERR_ARG,
                "n is not divisible by bs, n = " + std::to_string(A->n) + ", bs = " + std::to_string(bs));
   DECO_REQUIRE(prm.pressure_id >= 0 && prm.pressure_id < bs, DECO_ERR_ARG, "pressure_id out of range");
-  DECO_REQUIRE(prm.seq == 0 || prm.seq == 1 || prm.seq == 3, DECO_ERR_UNSUPPORTED,
-               "seq must be 0, 1 or 3 (seq 2 needs block Jacobi, not available on this path)");
+  DECO_REQUIRE(prm.seq >= 0 && prm.seq <= 3, DECO_ERR_ARG, "seq must be 0, 1, 2 or 3");
+  DECO_REQUIRE((prm.glo_type == 0 || prm.glo_type == 1) && (prm.loc_type == 0 || prm.loc_type == 1),
+               DECO_ERR_UNSUPPORTED, "prec_glo / prec_loc type must be FSAI or Jacobi on the GPU path");
   DECO_REQUIRE(prm.weights >= 0 && prm.weights <= 2, DECO_ERR_ARG, "weights must be 0, 1 or 2");
   DECO_REQUIRE(prm.precision == 64 || prm.precision == 32, DECO_ERR_ARG, "precision must be 64 or 32");
   P->prm = prm;
@@ -374,6 +417,8 @@ static void cpr_build(deco_ctx_s* ctx, deco_csr_s* A, double* d_b, const deco_cp
   Ev ev(ctx);
   P->J.alloc((size_t)P->sn * bs * bs, st);
   P->w.alloc(P->n, st);
+  P->w0.alloc(P->n, st);
+  P->ops.alloc(P->sn, st);
   P->check_diag.alloc(P->n, st);
   P->check_diag.zero(st);
   DevBuf<int> flags(2, st);
@@ -382,7 +427,7 @@ static void cpr_build(deco_ctx_s* ctx, deco_csr_s* A, double* d_b, const deco_cp
   a.sn = P->sn; a.bs = bs; a.pid = P->p; a.weights = prm.weights; a.use_drs = prm.use_drs; a.cpd = prm.cpd;
   a.e_dd = prm.drs_e_dd; a.e_ps = prm.drs_e_ps;
   a.r = A->r.get(); a.c = A->c.get(); a.v = A->v.get(); a.b = d_b;
-  a.w = P->w.get(); a.J = P->J.get(); a.chk = P->check_diag.get(); a.err = flags.get(); a.nfixed = flags.get() + 1;
+  a.w = P->w.get(); a.w0 = P->w0.get(); a.ops = P->ops.get(); a.J = P->J.get(); a.chk = P->check_diag.get(); a.err = flags.get(); a.nfixed = flags.get() + 1;
   cpr_decouple<<<grid_for(ctx, P->sn, 128, 16), 128, 0, st>>>(a);
   DECO_CHECK_LAUNCH();
   int hf[2];
@@ -412,16 +457,24 @@ static void cpr_build(deco_ctx_s* ctx, deco_csr_s* A, double* d_b, const deco_cp
     if (prm.loc_tol_rel > 1e-20) csr_filter_inplace(ctx, &P->Ap, prm.loc_tol_rel, 0.0);
   }
   P->t_ms[1] = ev.stop();
-  fsai_build(ctx, A, prm.glo_tol_rel, prm.glo_tol_abs, prm.glo_power, prm.precision, &P->glo);
+  const int jbs = prm.glo_block_size > 0 ? prm.glo_block_size : bs;
+  if (prm.glo_type == 1) jacobi_build(ctx, A, jbs, prm.precision, &P->jac);
+  else fsai_build(ctx, A, prm.glo_tol_rel, prm.glo_tol_abs, prm.glo_power, prm.precision, &P->glo, bs);
   P->t_ms[2] = ev.stop();
-  fsai_build(ctx, &P->Ap, prm.loc_tol_rel, prm.loc_tol_abs, prm.loc_power, prm.precision, &P->loc);
+  if (prm.loc_type == 1)
+    jacobi_build(ctx, &P->Ap, prm.loc_block_size > 0 ? prm.loc_block_size : 1, prm.precision, &P->jloc);
+  else fsai_build(ctx, &P->Ap, prm.loc_tol_rel, prm.loc_tol_abs, prm.loc_power, prm.precision, &P->loc);
   P->t_ms[3] = ev.stop();
+  // seq 2 with an FSAI global stage also builds the Jacobi of prec_glo (CPR.hpp:154-162)
+  if (prm.seq == 2 && prm.glo_type == 0) jacobi_build(ctx, A, jbs, prm.precision, &P->jac);
+  P->t_ms[0] += ev.stop();
   if (P->fixed)
     unfix_diag<<<grid_for(ctx, P->n, 256), 256, 0, st>>>(P->n, A->r.get(), A->c.get(), A->v.get(),
                                                          P->check_diag.get());
   DECO_CHECK_LAUNCH();
   P->rt.alloc(P->n, st);
   P->rts.alloc(P->sn, st);
+  make_bsr(ctx, A, bs);
   if (prm.precision == 32) {
     make_f32_values(ctx, A);
     P->rt32.alloc(P->n, st);
@@ -430,9 +483,29 @@ static void cpr_build(deco_ctx_s* ctx, deco_csr_s* A, double* d_b, const deco_cp
   // choose SpMV widths now, outside any later graph capture
   tuned_subwarp(ctx, A, false);
   if (prm.precision == 32) tuned_subwarp(ctx, A, true);
-  for (deco_csr_s* M : {&P->glo.FL, &P->glo.FUt, &P->loc.FL, &P->loc.FUt}) tuned_subwarp(ctx, M, prm.precision == 32);
+  for (deco_csr_s* M : {&P->glo.FL, &P->glo.FUt, &P->loc.FL, &P->loc.FUt})
+    if (M->n) tuned_subwarp(ctx, M, prm.precision == 32);
+  for (deco_csr_s* M : {A, &P->glo.FL, &P->glo.FUt})
+    if (M->bbs) {
+      tuned_bsr_subwarp(ctx, M, false);
+      if (prm.precision == 32) tuned_bsr_subwarp(ctx, M, true);
+    }
   DECO_CUDA(cudaStreamSynchronize(st));
   P->t_ms[4] = P->t_ms[0] + P->t_ms[1] + P->t_ms[2] + P->t_ms[3] + ev.stop();
+}
+
+// The global stage (FSAI, or Jacobi with prec_glo.type Jacobi) and the local
+// stage (FSAI or Jacobi on A_pp): epi(row, value) with value = (M in)[row].
+// alias: the reference calls this stage in place (precond_glo(rt, rt)).
+template <typename VT, typename XT, typename TT, class Epi>
+void glo_stage(deco_ctx_s* ctx, deco_cpr_s* P, const XT* in, TT* tmp, Epi epi, bool alias = false) {
+  if (P->prm.glo_type == 1) jacobi_apply<VT, XT>(ctx, &P->jac, in, epi, alias);
+  else fsai_apply_t<VT, XT, TT>(ctx, &P->glo, in, tmp, epi);
+}
+template <typename VT, typename XT, typename TT, class Epi>
+void loc_stage(deco_ctx_s* ctx, deco_cpr_s* P, const XT* in, TT* tmp, Epi epi) {
+  if (P->prm.loc_type == 1) jacobi_apply<VT, XT>(ctx, &P->jloc, in, epi);
+  else fsai_apply_t<VT, XT, TT>(ctx, &P->loc, in, tmp, epi);
 }
 
 void cpr_apply64(deco_ctx_s* ctx, deco_cpr_s* P, const double* r, double* x) {
@@ -442,22 +515,23 @@ void cpr_apply64(deco_ctx_s* ctx, deco_cpr_s* P, const double* r, double* x) {
     cudaStream_t st = ctx->stream;
     gather_pressure<double, double><<<grid_for(ctx, P->sn, 256), 256, 0, st>>>(P->sn, bs, p, r, P->rts.get());
     DECO_CHECK_LAUNCH();
-    fsai_apply_t<double, double, double>(ctx, &P->loc, P->rts.get(), P->loc.tmp.get(), EpiStore<double>{P->rts.get()});
+    loc_stage<double, double, double>(ctx, P, P->rts.get(), P->loc.tmp.get(), EpiStore<double>{P->rts.get()});
     scatter_pressure<double, double><<<grid_for(ctx, P->n, 256), 256, 0, st>>>(P->n, bs, p, P->rts.get(), x, 0);
     DECO_CHECK_LAUNCH();
     spmv<double, double>(ctx, A, x, EpiResid<double, double>{r, P->rt.get()});
-    fsai_apply_t<double, double, double>(ctx, &P->glo, P->rt.get(), P->glo.tmp.get(), EpiStore<double>{x});
+    glo_stage<double, double, double>(ctx, P, P->rt.get(), P->glo.tmp.get(), EpiStore<double>{x});
     scatter_pressure<double, double><<<grid_for(ctx, P->n, 256), 256, 0, st>>>(P->n, bs, p, P->rts.get(), x, 1);
     DECO_CHECK_LAUNCH();
     return;
   }
-  // seq 3 (and its first half, seq 0)
-  fsai_apply_t<double, double, double>(ctx, &P->glo, r, P->glo.tmp.get(), EpiStore<double>{x});
+  // seq 3 (and its first half, seq 0); seq 2 starts with the Jacobi stage
+  if (P->prm.seq == 2) jacobi_apply<double, double>(ctx, &P->jac, r, EpiStore<double>{x});
+  else glo_stage<double, double, double>(ctx, P, r, P->glo.tmp.get(), EpiStore<double>{x});
   spmv<double, double>(ctx, A, x, EpiRestrict<double, double>{r, P->rts.get(), bs, p}, bs);
-  fsai_apply_t<double, double, double>(ctx, &P->loc, P->rts.get(), P->loc.tmp.get(), EpiProlong<double>{x, bs, p});
+  loc_stage<double, double, double>(ctx, P, P->rts.get(), P->loc.tmp.get(), EpiProlong<double>{x, bs, p});
   if (P->prm.seq == 0) return;
   spmv<double, double>(ctx, A, x, EpiResid<double, double>{r, P->rt.get()});
-  fsai_apply_t<double, double, double>(ctx, &P->glo, P->rt.get(), P->glo.tmp.get(), EpiAdd<double>{x});
+  glo_stage<double, double, double>(ctx, P, P->rt.get(), P->glo.tmp.get(), EpiAdd<double>{x}, true);
 }
 
 template <typename RT, typename XT>
@@ -470,21 +544,22 @@ void cpr_apply32(deco_ctx_s* ctx, deco_cpr_s* P, const RT* r, XT* x) {
     cudaStream_t st = ctx->stream;
     gather_pressure<RT, float><<<grid_for(ctx, P->sn, 256), 256, 0, st>>>(P->sn, bs, p, r, P->rts32.get());
     DECO_CHECK_LAUNCH();
-    fsai_apply_t<float, float, float>(ctx, &P->loc, P->rts32.get(), tl, EpiStore<float>{P->rts32.get()});
+    loc_stage<float, float, float>(ctx, P, P->rts32.get(), tl, EpiStore<float>{P->rts32.get()});
     scatter_pressure<XT, float><<<grid_for(ctx, P->n, 256), 256, 0, st>>>(P->n, bs, p, P->rts32.get(), x, 0);
     DECO_CHECK_LAUNCH();
     spmv<float, XT>(ctx, A, x, EpiResid<RT, float>{r, P->rt32.get()});
-    fsai_apply_t<float, float, float>(ctx, &P->glo, P->rt32.get(), tg, EpiStore<XT>{x});
+    glo_stage<float, float, float>(ctx, P, P->rt32.get(), tg, EpiStore<XT>{x});
     scatter_pressure<XT, float><<<grid_for(ctx, P->n, 256), 256, 0, st>>>(P->n, bs, p, P->rts32.get(), x, 1);
     DECO_CHECK_LAUNCH();
     return;
   }
-  fsai_apply_t<float, RT, float>(ctx, &P->glo, r, tg, EpiStore<XT>{x});
+  if (P->prm.seq == 2) jacobi_apply<float, RT>(ctx, &P->jac, r, EpiStore<XT>{x});
+  else glo_stage<float, RT, float>(ctx, P, r, tg, EpiStore<XT>{x});
   spmv<float, XT>(ctx, A, x, EpiRestrict<RT, float>{r, P->rts32.get(), bs, p}, bs);
-  fsai_apply_t<float, float, float>(ctx, &P->loc, P->rts32.get(), tl, EpiProlong<XT>{x, bs, p});
+  loc_stage<float, float, float>(ctx, P, P->rts32.get(), tl, EpiProlong<XT>{x, bs, p});
   if (P->prm.seq == 0) return;
   spmv<float, XT>(ctx, A, x, EpiResid<RT, float>{r, P->rt32.get()});
-  fsai_apply_t<float, float, float>(ctx, &P->glo, P->rt32.get(), tg, EpiAdd<XT>{x});
+  glo_stage<float, float, float>(ctx, P, P->rt32.get(), tg, EpiAdd<XT>{x}, true);
 }
 
 template void cpr_apply32<double, double>(deco_ctx_s*, deco_cpr_s*, const double*, double*);
@@ -534,6 +609,8 @@ int deco_cpr_pressure(deco_cpr P, deco_csr* Ap) {
 int deco_cpr_fsai(deco_cpr P, int which, deco_fsai* F) {
   return guard([&] {
     DECO_REQUIRE(P && F && (which == 0 || which == 1), DECO_ERR_ARG, "bad argument");
+    DECO_REQUIRE((which == 0 ? P->prm.glo_type : P->prm.loc_type) == 0, DECO_ERR_ARG,
+                 "that stage is a Jacobi preconditioner, not an FSAI");
     *F = which == 0 ? &P->glo : &P->loc;
   });
 }
@@ -542,6 +619,16 @@ int deco_cpr_timings(deco_cpr P, double* ms5) {
   return guard([&] {
     DECO_REQUIRE(P && ms5, DECO_ERR_ARG, "NULL argument");
     for (int i = 0; i < 5; ++i) ms5[i] = P->t_ms[i];
+  });
+}
+
+int deco_cpr_decouple_rhs(deco_ctx ctx, deco_cpr P, double* d_b) {
+  return guard([&] {
+    DECO_REQUIRE(ctx && P && d_b, DECO_ERR_ARG, "NULL argument");
+    const deco_cpr_params& m = P->prm;
+    cpr_decouple_rhs<<<grid_for(ctx, P->sn, 256), 256, 0, ctx->stream>>>(
+        P->sn, P->bs, m.weights, m.use_drs, m.cpd, P->w0.get(), P->ops.get(), P->J.get(), d_b);
+    DECO_CHECK_LAUNCH();
   });
 }
 

@@ -1,14 +1,19 @@
 // cpr.cuh — CPR preconditioner handle and the templated apply used by GMRES.
 #pragma once
 #include "fsai.cuh"
+#include "jacobi.cuh"
 
 struct deco_cpr_s {
   deco_cpr_params prm{};
   int n = 0, sn = 0, bs = 1, p = 0;
   deco_csr_s* A = nullptr;        // the decoupled system (borrowed, mutated in place)
   deco_csr_s Ap;                  // pressure matrix A_pp
-  deco_fsai_s glo, loc;           // global FSAI on A, local FSAI on A_pp
+  deco_fsai_s glo, loc;           // global FSAI on A, local FSAI on A_pp (when their type is FSAI)
+  deco_jacobi_s jac;              // Jacobi on A: the global stage (type Jacobi) or seq 2's first stage
+  deco_jacobi_s jloc;             // Jacobi on A_pp (local type Jacobi)
   deco::DevBuf<double> J, w;      // CPD blocks, IMPES weights
+  deco::DevBuf<double> w0;        // weights before the DRS reset (right-hand-side replay)
+  deco::DevBuf<unsigned char> ops;  // per-cell DRS row flags and row swap (right-hand-side replay)
   deco::DevBuf<char> check_diag;  // rows whose diagonal fix_diag replaced
   deco::DevBuf<double> rt, rts;   // residual (n) and restricted residual (sn)
   deco::DevBuf<float> rt32, rts32;

@@ -1,6 +1,7 @@
 // csr.cu — device CSR matrices (deco_csr), the SpMV autotuner and the SpMV /
 // residual entry points of the C ABI.
 #include <algorithm>
+#include <climits>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -24,7 +25,91 @@ __global__ void to_f32(const double* __restrict__ a, float* __restrict__ b, long
     b[i] = (float)a[i];
 }
 
+// one thread per cell: the number of distinct block columns over its bs rows
+// (each row's columns are ascending, so its block columns are too)
+__global__ void bsr_count(int nbr, int bs, const int* __restrict__ r, const int* __restrict__ c,
+                          int* __restrict__ cnt) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nbr; s += gridDim.x * blockDim.x) {
+    int pos[3], end[3];
+    for (int q = 0; q < bs; ++q) { pos[q] = r[s * bs + q]; end[q] = r[s * bs + q + 1]; }
+    int k = 0;
+    for (;;) {
+      int mn = INT_MAX;
+      for (int q = 0; q < bs; ++q)
+        if (pos[q] < end[q]) mn = min(mn, c[pos[q]] / bs);
+      if (mn == INT_MAX) break;
+      ++k;
+      for (int q = 0; q < bs; ++q)
+        while (pos[q] < end[q] && c[pos[q]] / bs == mn) ++pos[q];
+    }
+    cnt[s] = k;
+  }
+}
+
+// the same merge, writing block columns and the values into their row planes
+// (bv is zero-filled beforehand: absent entries stay zero)
+__global__ void bsr_fill(int nbr, int bs, const int* __restrict__ r, const int* __restrict__ c,
+                         const double* __restrict__ v, const int* __restrict__ br, int* __restrict__ bc,
+                         double* __restrict__ bv, long long plane) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nbr; s += gridDim.x * blockDim.x) {
+    int pos[3], end[3];
+    for (int q = 0; q < bs; ++q) { pos[q] = r[s * bs + q]; end[q] = r[s * bs + q + 1]; }
+    int k = br[s];
+    for (;;) {
+      int mn = INT_MAX;
+      for (int q = 0; q < bs; ++q)
+        if (pos[q] < end[q]) mn = min(mn, c[pos[q]] / bs);
+      if (mn == INT_MAX) break;
+      bc[k] = mn;
+      for (int q = 0; q < bs; ++q)
+        for (; pos[q] < end[q] && c[pos[q]] / bs == mn; ++pos[q])
+          bv[q * plane + (long long)k * bs + c[pos[q]] % bs] = v[pos[q]];
+      ++k;
+    }
+  }
+}
+
 }  // namespace
+
+void drop_bsr(deco_csr_s* A) {
+  A->bbs = 0;
+  A->nblk = 0;
+  A->br = DevBuf<int>();
+  A->bc = DevBuf<int>();
+  A->bv = DevBuf<double>();
+  A->bv32 = DevBuf<float>();
+  A->bsw64 = A->bsw32 = 0;
+}
+
+void make_bsr(deco_ctx_s* ctx, deco_csr_s* A, int bs, double max_fill) {
+  drop_bsr(A);
+  if (!ctx->bsr || (bs != 2 && bs != 3) || A->n == 0 || A->n % bs || A->m % bs) return;
+  cudaStream_t st = ctx->stream;
+  const int nbr = A->n / bs;
+  DevBuf<int> cnt(nbr + 1, st);
+  const int g = grid_for(ctx, nbr, 256);
+  bsr_count<<<g, 256, 0, st>>>(nbr, bs, A->r.get(), A->c.get(), cnt.get());
+  DECO_CHECK_LAUNCH();
+  DevBuf<int> br(nbr + 1, st);
+  const long long nblk = exclusive_scan_int(ctx, cnt.get(), br.get(), nbr);
+  if ((double)nblk * bs * bs > max_fill * (double)A->nz) return;  // too much padding: keep CSR only
+  A->br = std::move(br);
+  A->nblk = (int)nblk;
+  A->bc.alloc(nblk, st);
+  const long long plane = nblk * bs;
+  A->bv.alloc(plane * bs, st);
+  A->bv.zero(st);
+  bsr_fill<<<g, 256, 0, st>>>(nbr, bs, A->r.get(), A->c.get(), A->v.get(), A->br.get(), A->bc.get(), A->bv.get(),
+                              plane);
+  DECO_CHECK_LAUNCH();
+  A->bbs = bs;
+  A->avg_blk = double(nblk) / nbr;
+  if (A->v32) {
+    A->bv32.alloc(plane * bs, st);
+    to_f32<<<grid_for(ctx, plane * bs, 256), 256, 0, st>>>(A->bv.get(), A->bv32.get(), plane * bs);
+    DECO_CHECK_LAUNCH();
+  }
+}
 
 void refresh_stats(deco_ctx_s* ctx, deco_csr_s* A) {
   DevBuf<int> mx(1, ctx->stream);
@@ -35,18 +120,76 @@ void refresh_stats(deco_ctx_s* ctx, deco_csr_s* A) {
   DECO_CUDA(cudaStreamSynchronize(ctx->stream));
   A->avg_row = A->n ? double(A->nz) / A->n : 0.0;
   A->sw64 = A->sw32 = 0;
+  A->bsw64 = A->bsw32 = 0;
 }
 
 void make_f32_values(deco_ctx_s* ctx, deco_csr_s* A) {
   if (!A->v32 || A->v32.size() != (size_t)A->nz) A->v32.alloc(A->nz, ctx->stream);
   to_f32<<<grid_for(ctx, A->nz, 256), 256, 0, ctx->stream>>>(A->v.get(), A->v32.get(), A->nz);
   DECO_CHECK_LAUNCH();
+  if (A->bbs) {
+    const long long nv = (long long)A->nblk * A->bbs * A->bbs;
+    if (!A->bv32 || A->bv32.size() != (size_t)nv) A->bv32.alloc(nv, ctx->stream);
+    to_f32<<<grid_for(ctx, nv, 256), 256, 0, ctx->stream>>>(A->bv.get(), A->bv32.get(), nv);
+    DECO_CHECK_LAUNCH();
+  }
 }
 
 // process-wide cache of tuned widths, keyed by the matrix's shape, so a freshly
 // assembled system with the same structure is not timed again
 static std::map<std::tuple<int, int, int, int, bool>, int> g_tuned;
 static std::mutex g_tuned_mu;
+
+int tuned_bsr_subwarp(deco_ctx_s* ctx, deco_csr_s* A, bool f32) {
+  int& sw = f32 ? A->bsw32 : A->bsw64;
+  if (sw) return sw;
+  sw = 1;
+  while (sw < 16 && sw < A->avg_blk / 2.0) sw <<= 1;
+  const int nbr = A->n / A->bbs;
+  if (!ctx->autotune || nbr < 4096) return sw;
+  const auto key = std::make_tuple(A->n, A->m, A->nblk, -A->bbs, f32);
+  {
+    std::lock_guard<std::mutex> lk(g_tuned_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) return sw = it->second;
+  }
+  cudaStreamCaptureStatus cs;
+  DECO_CUDA(cudaStreamIsCapturing(ctx->stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return sw;
+  DevBuf<double> x(A->m, ctx->stream), y(A->n, ctx->stream);
+  DevBuf<float> xf, yf;
+  x.zero(ctx->stream);
+  if (f32) { xf.alloc(A->m, ctx->stream); yf.alloc(A->n, ctx->stream); xf.zero(ctx->stream); }
+  auto time_width = [&](int cand) {
+    float t[5];
+    for (int rep = 0; rep < 6; ++rep) {
+      DECO_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+      if (f32) launch_bsr<float, float>(ctx->stream, A, cand, false, xf.get(), EpiStore<float>{yf.get()});
+      else launch_bsr<double, double>(ctx->stream, A, cand, false, x.get(), EpiStore<double>{y.get()});
+      DECO_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+      DECO_CUDA(cudaEventSynchronize(ctx->ev1));
+      float ms = 0.f;
+      DECO_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+      if (rep > 0) t[rep - 1] = ms;
+    }
+    std::sort(t, t + 5);
+    return t[2];
+  };
+  const int base = sw;
+  const float t_base = time_width(base);
+  float best = t_base;
+  int best_sw = base;
+  for (int cand : {base / 2, base * 2}) {
+    if (cand < 1 || cand > 16) continue;
+    const float tc = time_width(cand);
+    if (tc < best) { best = tc; best_sw = cand; }
+  }
+  if (best > 0.95f * t_base) best_sw = base;
+  sw = best_sw;
+  std::lock_guard<std::mutex> lk(g_tuned_mu);
+  g_tuned[key] = sw;
+  return sw;
+}
 
 int tuned_subwarp(deco_ctx_s* ctx, deco_csr_s* A, bool f32) {
   int& sw = f32 ? A->sw32 : A->sw64;
@@ -165,6 +308,7 @@ int deco_csr_set_values(deco_ctx ctx, deco_csr A, const double* v, int where) {
     DECO_REQUIRE(ctx && A && v, DECO_ERR_ARG, "NULL argument");
     DECO_CUDA(cudaMemcpyAsync(A->v.get(), v, sizeof(double) * (size_t)A->nz,
                               where ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+    if (A->bbs) make_bsr(ctx, A, A->bbs);
     if (A->v32) make_f32_values(ctx, A);
   });
 }
@@ -190,6 +334,24 @@ int deco_csr_set_subwarp(deco_csr A, int sw) {
                  "sub-warp width must be a power of two in [1, 32]");
     A->sw64 = sw;
     A->sw32 = sw;
+  });
+}
+
+int deco_csr_set_blocks(deco_ctx ctx, deco_csr A, int bs) {
+  return guard([&] {
+    DECO_REQUIRE(ctx && A, DECO_ERR_ARG, "NULL argument");
+    DECO_REQUIRE(bs == 0 || bs == 2 || bs == 3, DECO_ERR_ARG, "block size must be 0, 2 or 3");
+    DECO_REQUIRE(bs == 0 || (A->n % bs == 0 && A->m % bs == 0), DECO_ERR_ARG, "n and m must be multiples of bs");
+    if (bs == 0) drop_bsr(A);
+    else make_bsr(ctx, A, bs);
+  });
+}
+
+int deco_csr_blocks(deco_csr A, int* bs, int* nblk) {
+  return guard([&] {
+    DECO_REQUIRE(A, DECO_ERR_ARG, "A is NULL");
+    if (bs) *bs = A->bbs;
+    if (nblk) *nblk = A->nblk;
   });
 }
 

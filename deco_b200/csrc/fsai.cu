@@ -500,6 +500,7 @@ void csr_filter(deco_ctx_s* ctx, const deco_csr_s* A, double tol_rel, double tol
 void csr_filter_inplace(deco_ctx_s* ctx, deco_csr_s* A, double tol_rel, double tol_abs) {
   deco_csr_s B;
   csr_filter(ctx, A, tol_rel, tol_abs, &B);
+  drop_bsr(A);
   A->nz = B.nz;
   A->r = std::move(B.r);
   A->c = std::move(B.c);
@@ -508,8 +509,34 @@ void csr_filter_inplace(deco_ctx_s* ctx, deco_csr_s* A, double tol_rel, double t
   refresh_stats(ctx, A);
 }
 
+void csr_transpose(deco_ctx_s* ctx, int n, int m, int nz, const int* r, const int* c, const double* v,
+                   deco_csr_s* T) {
+  cudaStream_t st = ctx->stream;
+  T->n = m;
+  T->m = n;
+  T->nz = nz;
+  DevBuf<int> ccount(m + 1, st);
+  ccount.zero(st);
+  if (nz) {
+    col_count<<<grid_for(ctx, nz, 256), 256, 0, st>>>(nz, c, ccount.get());
+    DECO_CHECK_LAUNCH();
+  }
+  T->r.alloc(m + 1, st);
+  exclusive_scan_int(ctx, ccount.get(), T->r.get(), m);
+  T->c.alloc(nz, st);
+  T->v.alloc(nz, st);
+  if (nz) {
+    DECO_CUDA(cudaMemcpyAsync(ccount.get(), T->r.get(), sizeof(int) * m, cudaMemcpyDeviceToDevice, st));
+    col_scatter<<<grid_for(ctx, n, 256), 256, 0, st>>>(n, r, c, v, ccount.get(), T->c.get(), T->v.get());
+    DECO_CHECK_LAUNCH();
+    sort_rows<<<grid_for(ctx, m, 256), 256, 0, st>>>(m, T->r.get(), T->c.get(), T->v.get());
+    DECO_CHECK_LAUNCH();
+  }
+  refresh_stats(ctx, T);
+}
+
 void fsai_build(deco_ctx_s* ctx, const deco_csr_s* A0, double tol_rel, double tol_abs, int power, int precision,
-                deco_fsai_s* F) {
+                deco_fsai_s* F, int bs) {
   cudaStream_t st = ctx->stream;
   DECO_REQUIRE(A0->n == A0->m, DECO_ERR_ARG, "FSAI needs a square matrix");
   DECO_REQUIRE(power == 1, DECO_ERR_UNSUPPORTED, "FSAI power 2 (lower(A^2) pattern) is not available on the GPU path");
@@ -574,23 +601,12 @@ void fsai_build(deco_ctx_s* ctx, const deco_csr_s* A0, double tol_rel, double to
   DECO_CHECK_LAUNCH();
   // 5. FU^T (trans_mat_full)
   deco_csr_s& U = F->FUt;
-  U.n = U.m = n;
-  U.nz = FL.nz;
-  DevBuf<int> ccount(n + 1, st);
-  ccount.zero(st);
-  col_count<<<grid_for(ctx, FL.nz, 256), 256, 0, st>>>(FL.nz, FL.c.get(), ccount.get());
-  DECO_CHECK_LAUNCH();
-  U.r.alloc(n + 1, st);
-  exclusive_scan_int(ctx, ccount.get(), U.r.get(), n);
-  U.c.alloc(U.nz, st);
-  U.v.alloc(U.nz, st);
-  DECO_CUDA(cudaMemcpyAsync(ccount.get(), U.r.get(), sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
-  col_scatter<<<g, 256, 0, st>>>(n, FL.r.get(), FL.c.get(), fu.get(), ccount.get(), U.c.get(), U.v.get());
-  DECO_CHECK_LAUNCH();
-  sort_rows<<<g, 256, 0, st>>>(n, U.r.get(), U.c.get(), U.v.get());
-  DECO_CHECK_LAUNCH();
+  csr_transpose(ctx, n, n, FL.nz, FL.r.get(), FL.c.get(), fu.get(), &U);
   refresh_stats(ctx, &FL);
-  refresh_stats(ctx, &U);
+  if (bs > 1) {
+    make_bsr(ctx, &FL, bs);
+    make_bsr(ctx, &U, bs);
+  }
   F->tmp.alloc(n, st);
   if (precision == 32) {
     make_f32_values(ctx, &FL);
@@ -631,6 +647,15 @@ int deco_fsai_info(deco_fsai F, int* n, int* nz, int* max_order) {
     if (n) *n = F->n;
     if (nz) *nz = F->nz;
     if (max_order) *max_order = F->max_order;
+  });
+}
+
+int deco_fsai_blocks(deco_fsai F, int* bs, int* nblk_lower, int* nblk_upper) {
+  return guard([&] {
+    DECO_REQUIRE(F, DECO_ERR_ARG, "F is NULL");
+    if (bs) *bs = F->FL.bbs;
+    if (nblk_lower) *nblk_lower = F->FL.nblk;
+    if (nblk_upper) *nblk_upper = F->FUt.nblk;
   });
 }
 

@@ -21,8 +21,9 @@ void csr_filter(deco_ctx_s* ctx, const deco_csr_s* A, double tol_rel, double tol
 void csr_filter_inplace(deco_ctx_s* ctx, deco_csr_s* A, double tol_rel, double tol_abs);
 
 // FSAI setup on a device matrix (the setup always runs in float64).
+// bs > 1: the factors also get cell-block copies (make_bsr) for their products.
 void fsai_build(deco_ctx_s* ctx, const deco_csr_s* A, double tol_rel, double tol_abs, int power, int precision,
-                deco_fsai_s* F);
+                deco_fsai_s* F, int bs = 1);
 
 // y = FU^T (FL x) with fused epilogue on the second product.
 template <typename VT, typename XT, typename TT, class Epi>
@@ -30,6 +31,11 @@ void fsai_apply_t(deco_ctx_s* ctx, deco_fsai_s* F, const XT* x, TT* tmp, Epi epi
   spmv<VT, XT>(ctx, &F->FL, x, EpiStore<TT>{tmp});
   spmv<VT, TT>(ctx, &F->FUt, tmp, epi);
 }
+
+// T = A^T for the n x m CSR (r, c, v): atomic column scatter, then every row of
+// T sorted by source row, so the result does not depend on scheduling.
+void csr_transpose(deco_ctx_s* ctx, int n, int m, int nz, const int* r, const int* c, const double* v,
+                   deco_csr_s* T);
 
 void refresh_stats(deco_ctx_s* ctx, deco_csr_s* A);
 void make_f32_values(deco_ctx_s* ctx, deco_csr_s* A);

@@ -300,7 +300,19 @@ int deco_gen_size(const deco_gen_params* p, int* n, long long* nnz) {
   return 0;
 }
 
-int deco_gen_fill(const deco_gen_params* p, int* r, int* c, double* v, double* b, double* logk) {
+}  // extern "C"
+
+namespace {
+
+// Assembly of the whole system, in one of two modes:
+//   fill      (dLdA == nullptr): writes r, c, v (and b, logk_out when non-null);
+//   gradient  (dLdA != nullptr): accumulates dL/d ln k[cell] from dL/dA on the
+//             pattern into dLdlogk, using that every entry that depends on a
+//             face transmissibility T is T times a coefficient independent of k,
+//             and dT/d ln k_a = T k_b / (k_a + k_b) for T = 2 k_a k_b/(k_a+k_b) * mult.
+// logk_in == nullptr generates the seeded field; otherwise it is used as given.
+int assemble(const deco_gen_params* p, const double* logk_in, int* r, int* c, double* v, double* b,
+             double* logk_out, const double* dLdA, double* dLdlogk) {
   int e = validate(p);
   if (e) return e;
   int n;
@@ -310,10 +322,12 @@ int deco_gen_fill(const deco_gen_params* p, int* r, int* c, double* v, double* b
   s.p = p; s.nx = p->nx; s.ny = p->ny; s.nz = p->nz; s.bs = p->bs;
   s.nc = (long long)p->nx * p->ny * p->nz;
   build_faults(s);
-  build_logk(s);
+  if (logk_in) s.logk.assign(logk_in, logk_in + s.nc);
+  else build_logk(s);
   build_wells(s);
   const int bs = s.bs;
   const long long nc = s.nc;
+  const bool grad = dLdA != nullptr;
 
   // row pointers: every row of a cell has bs * |neighbours| entries
   std::vector<long long> cstart(nc + 1, 0);
@@ -324,6 +338,10 @@ int deco_gen_fill(const deco_gen_params* p, int* r, int* c, double* v, double* b
   }
   for (long long i = 0; i < nc; ++i) cstart[i + 1] += cstart[i];
   if (cstart[nc] * bs * bs != nnz) return -6;
+  // gradient mode: the neighbour side of each face, written per (cell, slot), summed after
+  std::vector<double> nbpart(grad ? cstart[nc] : 0, 0.0);
+  if (grad)
+    for (long long i = 0; i < nc; ++i) dLdlogk[i] = 0.0;
 
 #pragma omp parallel for schedule(static, 256)
   for (long long ci = 0; ci < nc; ++ci) {
@@ -332,17 +350,22 @@ int deco_gen_fill(const deco_gen_params* p, int* r, int* c, double* v, double* b
     const int m = neighbours(s, cs, nb);
     const long long rowlen = (long long)m * bs;
     const long long base = cstart[ci] * bs * bs;  // first entry of row cs*bs
-    for (int a = 0; a < bs; ++a) r[(long long)cs * bs + a] = int(base + a * rowlen);
-    if (ci == nc - 1) r[n] = int(base + bs * rowlen);
+    if (!grad) {
+      for (int a = 0; a < bs; ++a) r[(long long)cs * bs + a] = int(base + a * rowlen);
+      if (ci == nc - 1) r[n] = int(base + bs * rowlen);
+    }
+    int self = -1;
+    for (int q = 0; q < m; ++q)
+      if (nb[q] == cs) self = q;
 
     double D[3][3] = {{0}};
     double O[64][3][3];
     const CellData me = cell_data(s, cs);
     const double ks = std::exp(s.logk[ci]);
-    int self = -1;
+    double gself = 0.0;
     for (int q = 0; q < m; ++q) {
       const int t = nb[q];
-      if (t == cs) { self = q; continue; }
+      if (t == cs) continue;
       const int fa = std::min(cs, t), fb = std::max(cs, t);
       const uint64_t fid = (uint64_t)fa * 2654435761ull ^ ((uint64_t)fb << 20) ^ (uint64_t)fb;
       const double kt = std::exp(s.logk[t]);
@@ -351,24 +374,53 @@ int deco_gen_fill(const deco_gen_params* p, int* r, int* c, double* v, double* b
       const int up = potential(s, fa) > potential(s, fb) ? fa : fb;
       const double g = logu(p->cpl_lo, p->cpl_hi, uni(p->seed, S_FACE_G, fid));
       const CellData ud = (up == cs) ? me : cell_data(s, up);
-      double (*Ob)[3] = O[q];
-      // pressure columns
-      Ob[0][0] = -T;
-      D[0][0] += T;
-      for (int a = 1; a < bs; ++a) { Ob[a][0] = -T * ud.fr[a]; D[a][0] += T * ud.fr[a]; }
-      // saturation columns (upwinded)
+      if (!grad) {
+        double (*Ob)[3] = O[q];
+        // pressure columns
+        Ob[0][0] = -T;
+        D[0][0] += T;
+        for (int a = 1; a < bs; ++a) { Ob[a][0] = -T * ud.fr[a]; D[a][0] += T * ud.fr[a]; }
+        // saturation columns (upwinded)
+        for (int a = 0; a < bs; ++a)
+          for (int bb = 1; bb < bs; ++bb) {
+            double cab = (a == 0) ? 0.1 * T * g : (a == bb ? T * g : -0.3 * T * g);
+            if (up == cs) {
+              D[a][bb] += cab;
+              Ob[a][bb] = 1e-3 * cab;  // the non-upwind side keeps a tiny entry
+            } else {
+              Ob[a][bb] = -cab;
+            }
+          }
+        continue;
+      }
+      // gradient: the same entries divided by T (off-diagonal block kO, diagonal-block part kD)
+      double kO[3][3] = {{0}}, kD[3][3] = {{0}};
+      kO[0][0] = -1.0;
+      kD[0][0] = 1.0;
+      for (int a = 1; a < bs; ++a) { kO[a][0] = -ud.fr[a]; kD[a][0] = ud.fr[a]; }
       for (int a = 0; a < bs; ++a)
         for (int bb = 1; bb < bs; ++bb) {
-          double cab = (a == 0) ? 0.1 * T * g : (a == bb ? T * g : -0.3 * T * g);
+          const double kab = (a == 0) ? 0.1 * g : (a == bb ? g : -0.3 * g);
           if (up == cs) {
-            D[a][bb] += cab;
-            Ob[a][bb] = 1e-3 * cab;  // non-upwind side keeps a tiny entry
+            kD[a][bb] = kab;
+            kO[a][bb] = 1e-3 * kab;
           } else {
-            Ob[a][bb] = -cab;
+            kO[a][bb] = -kab;
           }
         }
+      double G = 0.0;  // dL/dT of this face through row block cs
+      for (int a = 0; a < bs; ++a) {
+        const double* row = dLdA + base + a * rowlen;
+        for (int bb = 0; bb < bs; ++bb) G += row[q * bs + bb] * kO[a][bb] + row[self * bs + bb] * kD[a][bb];
+      }
+      gself += G * T * kt / (ks + kt);
+      nbpart[cstart[ci] + q] = G * T * ks / (ks + kt);
     }
-    // accumulation, compressibility, wells
+    if (grad) {
+      dLdlogk[ci] += gself;
+      continue;
+    }
+    // accumulation, compressibility, wells (independent of k)
     D[0][0] += p->comp;
     for (int a = 1; a < bs; ++a) {
       D[a][a] += me.acc;
@@ -395,9 +447,36 @@ int deco_gen_fill(const deco_gen_params* p, int* r, int* c, double* v, double* b
       }
     }
   }
+  if (grad) {  // the neighbour halves, in cell order (deterministic)
+    for (long long ci = 0; ci < nc; ++ci) {
+      int nb[64];
+      const int m = neighbours(s, int(ci), nb);
+      for (int q = 0; q < m; ++q)
+        if (nb[q] != ci) dLdlogk[nb[q]] += nbpart[cstart[ci] + q];
+    }
+    return 0;
+  }
   if (b) deco_gen_uniform(p->seed, S_RHS, n, b);
-  if (logk) std::memcpy(logk, s.logk.data(), sizeof(double) * nc);
+  if (logk_out) std::memcpy(logk_out, s.logk.data(), sizeof(double) * nc);
   return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int deco_gen_fill(const deco_gen_params* p, int* r, int* c, double* v, double* b, double* logk) {
+  return assemble(p, nullptr, r, c, v, b, logk, nullptr, nullptr);
+}
+
+int deco_gen_fill_logk(const deco_gen_params* p, const double* logk, int* r, int* c, double* v, double* b) {
+  if (!logk) return -1;
+  return assemble(p, logk, r, c, v, b, nullptr, nullptr, nullptr);
+}
+
+int deco_gen_grad_logk(const deco_gen_params* p, const double* logk, const double* dLdA, double* dLdlogk) {
+  if (!dLdA || !dLdlogk) return -1;
+  return assemble(p, logk, nullptr, nullptr, nullptr, nullptr, nullptr, dLdA, dLdlogk);
 }
 
 void deco_gen_uniform(unsigned long long seed, unsigned long long stream, long long n, double* out) {

@@ -23,6 +23,7 @@
 // Precision 32: V, w, z in float32 with float64 accumulation; H, G, g and the
 // rotations in float64; every restart recomputes the true residual b - A x and
 // the solution update in float64 (iterative refinement).
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <vector>
@@ -37,7 +38,10 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kColsPerWarp = 8;
 constexpr int kMaxCols = kWarps * kColsPerWarp;  // basis columns pass A handles (restart <= 63)
-constexpr int kRowsPerLane = 8;                   // rows per lane per step of pass A
+// host read-back of |g_{j+1}|: a ring of kRing pinned slots (from kSlot0) and
+// events; the host runs up to `lookahead` Arnoldi steps ahead (<= kRing - 2)
+constexpr int kRing = 8;
+constexpr int kSlot0 = 4;
 constexpr double kEps = 2.220446049250312e-16;
 
 // device state (float64): H (m+1)*m | G (m+1)^2 | g | cs | sn | s | c | sums 2(m+2) | sc
@@ -64,8 +68,6 @@ struct State {
 };
 enum { SC_RES = 0, SC_BREAK = 1, SC_BETA = 2 };
 
-__device__ __forceinline__ double ldv(const double* p) { return __ldcs(p); }
-__device__ __forceinline__ double ldv(const float* p) { return (double)__ldcs(p); }
 
 // deterministic last-block reduction of red[i*nb + b] over b for i < ncols
 __device__ void finalize_partials(const double* red, int nb, int ncols, double* out) {
@@ -382,6 +384,7 @@ struct Solver {
   State st{};
   // DECO_PROFILE=1: events around the phases of every Arnoldi step of a cycle
   bool profile = false;
+  int lookahead = 3;  // Arnoldi steps queued beyond the one whose |g| the host is waiting for
   std::vector<cudaEvent_t> pev;
   double t_phase[3] = {0, 0, 0};
   ~Solver() {
@@ -405,6 +408,7 @@ struct Solver {
     const size_t need = (size_t)(2 * (m + 2)) * nb;
     if (ctx->red.size() < need) ctx->red.alloc(need, s);
     if (const char* e = std::getenv("DECO_PROFILE")) profile = std::atoi(e) != 0;
+    if (const char* e = std::getenv("DECO_LOOKAHEAD")) lookahead = std::max(0, std::min(kRing - 2, std::atoi(e)));
     if (profile) {
       pev.resize(4 * (size_t)(m + 1));
       for (auto& e : pev) DECO_CUDA(cudaEventCreate(&e));
@@ -463,7 +467,7 @@ struct Solver {
   }
 
   // Arnoldi step j: writes column j of H/G, g_{j+1}, rotation j and basis column
-  // j+1; |g_{j+1}| is copied to host slot (j & 1) and ev[j & 1] recorded after it.
+  // j+1; |g_{j+1}| is copied to host slot j % kRing and ev[j % kRing] recorded after it.
   void arnoldi_step(int j, bool left, volatile double* hsc, cudaEvent_t* ev) {
     cudaStream_t s = ctx->stream;
     const double* sj = st.s + j;
@@ -487,9 +491,9 @@ struct Solver {
                                               ctx->counter.get(), st);
     DECO_CHECK_LAUNCH();
     if (profile) DECO_CUDA(cudaEventRecord(pev[4 * j + 3], s));
-    DECO_CUDA(cudaMemcpyAsync(const_cast<double*>(hsc) + (j & 1), st.sc + SC_RES, sizeof(double),
+    DECO_CUDA(cudaMemcpyAsync(const_cast<double*>(hsc) + kSlot0 + j % kRing, st.sc + SC_RES, sizeof(double),
                               cudaMemcpyDeviceToHost, s));
-    DECO_CUDA(cudaEventRecord(ev[j & 1], s));
+    DECO_CUDA(cudaEventRecord(ev[j % kRing], s));
   }
 
   void run(const double* b, double* x, deco_sol_result* res, double* resvec) {
@@ -511,12 +515,13 @@ struct Solver {
     int flag = 1, iter = 0, restarts = 0;
     double rnorm = 0.0;
     volatile double* hsc = ctx->host_scalars;
-    cudaEvent_t ev[2];
-    DECO_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
-    DECO_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    cudaEvent_t ev[kRing];
+    for (auto& e : ev) DECO_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     struct EvGuard {
       cudaEvent_t* e;
-      ~EvGuard() { cudaEventDestroy(e[0]); cudaEventDestroy(e[1]); }
+      ~EvGuard() {
+        for (int i = 0; i < kRing; ++i) cudaEventDestroy(e[i]);
+      }
     } evg{ev};
     while (iter < itmax) {
       DECO_CUDA(cudaMemsetAsync(st_buf.get(), 0, sizeof(double) * State::doubles(m), s));
@@ -524,35 +529,31 @@ struct Solver {
       DECO_CHECK_LAUNCH();
       DECO_CUDA(cudaMemcpyAsync(const_cast<double*>(hsc) + 2, norm.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
       DECO_CUDA(cudaStreamSynchronize(s));
-      double gj = hsc[2];
-      bool known = true;  // |g_j| is on the host; otherwise it is in flight from step j-1
+      // The reference's loop (rgmres.tpp:58-66) checks |g_j| before Arnoldi step j.
+      // Here the host keeps up to `lookahead` steps queued past the |g_j| it is
+      // checking, so a late host thread does not leave the GPU idle.  When |g_j|
+      // meets the tolerance, steps j.. are dropped: step k wrote only column k of
+      // H/G, g_{k+1}, rotation k and basis column k+1, which the back substitution
+      // over j columns never reads.
+      const int base = iter;
       int j = 0, launched = 0;
       for (;;) {
-        // the reference's loop bounds and inner convergence check (rgmres.tpp:58-66)
-        if (!(j < m && iter < itmax)) break;
-        if (known) {
-          rnorm = fabs(gj);
-          if (resvec) resvec[iter] = rnorm / bnorm;
-          if (rnorm < abstol) { flag = 0; break; }
-          arnoldi_step(j, left, hsc, ev);
-          launched = j + 1;
-        } else {
-          // enqueue step j before looking at |g_j| from step j-1; if |g_j| already
-          // meets the tolerance, step j is dropped: it wrote only column j of H/G,
-          // g_{j+1}, rotation j and basis column j+1, which the back substitution
-          // over j columns never reads
-          arnoldi_step(j, left, hsc, ev);
-          launched = j + 1;
-          DECO_CUDA(cudaEventSynchronize(ev[(j - 1) & 1]));
-          gj = hsc[(j - 1) & 1];
-          rnorm = fabs(gj);
-          if (resvec) resvec[iter] = rnorm / bnorm;
-          if (rnorm < abstol) { flag = 0; break; }
+        if (!(j < m && base + j < itmax)) break;
+        double gj = hsc[2];  // |g_0|; step 0 is launched only after it is checked
+        if (j > 0) {
+          DECO_CUDA(cudaEventSynchronize(ev[(j - 1) % kRing]));
+          gj = hsc[kSlot0 + (j - 1) % kRing];
+        }
+        rnorm = fabs(gj);
+        if (resvec) resvec[base + j] = rnorm / bnorm;
+        if (rnorm < abstol) { flag = 0; break; }
+        while (launched < m && base + launched < itmax && launched <= j + lookahead) {
+          arnoldi_step(launched, left, hsc, ev);
+          ++launched;
         }
         ++j;
-        ++iter;
-        known = false;
       }
+      iter = base + j;
       backsolve<<<1, 1, 0, s>>>(st, j);
       DECO_CHECK_LAUNCH();
       DECO_CUDA(cudaMemcpyAsync(const_cast<double*>(hsc) + 3, st.sc + SC_BREAK, sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -27,6 +27,17 @@ struct deco_csr_s {
   int sw64 = 0, sw32 = 0;   // sub-warp width per value precision (0 = not chosen yet)
   int max_row = 0;
   double avg_row = 0;
+  // Cell-block copy for matrices of bs x bs cell blocks (reservoir systems):
+  // one column index per block instead of per entry, entries the CSR pattern
+  // lacks stored as zeros, and the values kept as bs row planes (plane q holds
+  // in-block row q of every block) so a product over row 0 of each cell reads
+  // one plane only.  bbs == 0: no block copy.
+  int bbs = 0, nblk = 0;
+  deco::DevBuf<int> br, bc;   // block-row pointers (n / bbs + 1), block columns
+  deco::DevBuf<double> bv;    // bbs planes of nblk * bbs values
+  deco::DevBuf<float> bv32;
+  int bsw64 = 0, bsw32 = 0;
+  double avg_blk = 0;
 };
 
 namespace deco {
@@ -126,6 +137,102 @@ void launch_spmv_sw(cudaStream_t st, int sw, int nrows_out, int row_stride, cons
   DECO_CHECK_LAUNCH();
 }
 
+// ------------------------------------------------------- cell-block kernel
+// A sub-warp of SW lanes owns a block row (one cell: BS matrix rows); each lane
+// takes whole blocks: one 4-byte block column, the BS x values of that cell (a
+// single 8/16-byte pair load for BS == 2) and BS values per computed row.  ROW0
+// computes only in-block row 0 of every cell (the restricted product of
+// alg::spmv with bs > 1) and reads only that value plane.
+template <typename T> struct Pair;
+template <> struct Pair<double> { using V = double2; };
+template <> struct Pair<float> { using V = float2; };
+
+template <int SW, int BS, bool ROW0, typename VT, typename XT, class Epi>
+__global__ void __launch_bounds__(256) bsr_kernel(int nbr, const int* __restrict__ br, const int* __restrict__ bc,
+                                                  const VT* __restrict__ bv, long long plane,
+                                                  const XT* __restrict__ x, Epi epi) {
+  constexpr int NR = ROW0 ? 1 : BS;
+  const int lane = threadIdx.x & (SW - 1);
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = int(gid / SW);
+  const bool valid = s < nbr;
+  double sum[NR];
+#pragma unroll
+  for (int q = 0; q < NR; ++q) sum[q] = 0.0;
+  if (valid) {
+    const int a = __ldg(br + s), e = __ldg(br + s + 1);
+    for (int k = a + lane; k < e; k += SW) {
+      const long long j = (long long)__ldcs(bc + k) * BS;
+      double xv[BS];
+      if constexpr (BS == 2) {
+        const typename Pair<XT>::V p = __ldg(reinterpret_cast<const typename Pair<XT>::V*>(x + j));
+        xv[0] = (double)p.x;
+        xv[1] = (double)p.y;
+      } else {
+#pragma unroll
+        for (int t = 0; t < BS; ++t) xv[t] = (double)__ldg(x + j + t);
+      }
+#pragma unroll
+      for (int q = 0; q < NR; ++q) {
+        const VT* vp = bv + q * plane + (long long)k * BS;
+        if constexpr (BS == 2) {
+          const typename Pair<VT>::V w = __ldcs(reinterpret_cast<const typename Pair<VT>::V*>(vp));
+          sum[q] += (double)w.x * xv[0];
+          sum[q] += (double)w.y * xv[1];
+        } else {
+#pragma unroll
+          for (int t = 0; t < BS; ++t) sum[q] += (double)__ldcs(vp + t) * xv[t];
+        }
+      }
+    }
+  }
+  if (SW > 1) {
+#pragma unroll
+    for (int q = 0; q < NR; ++q) sum[q] = subwarp_sum<SW>(sum[q]);
+  }
+  if (valid && lane == 0) {
+    if (ROW0) {
+      epi(s, sum[0]);
+    } else {
+#pragma unroll
+      for (int q = 0; q < NR; ++q) epi(s * BS + q, sum[q]);
+    }
+  }
+}
+
+template <int BS, bool ROW0, typename VT, typename XT, class Epi>
+void launch_bsr_bs(cudaStream_t st, int sw, int nbr, const int* br, const int* bc, const VT* bv, long long plane,
+                   const XT* x, Epi epi) {
+  const int block = 256;
+  const unsigned grid = (unsigned)cdiv((long long)nbr * sw, block);
+  switch (sw) {
+    case 1: bsr_kernel<1, BS, ROW0, VT, XT, Epi><<<grid, block, 0, st>>>(nbr, br, bc, bv, plane, x, epi); break;
+    case 2: bsr_kernel<2, BS, ROW0, VT, XT, Epi><<<grid, block, 0, st>>>(nbr, br, bc, bv, plane, x, epi); break;
+    case 4: bsr_kernel<4, BS, ROW0, VT, XT, Epi><<<grid, block, 0, st>>>(nbr, br, bc, bv, plane, x, epi); break;
+    case 8: bsr_kernel<8, BS, ROW0, VT, XT, Epi><<<grid, block, 0, st>>>(nbr, br, bc, bv, plane, x, epi); break;
+    default: bsr_kernel<16, BS, ROW0, VT, XT, Epi><<<grid, block, 0, st>>>(nbr, br, bc, bv, plane, x, epi); break;
+  }
+  DECO_CHECK_LAUNCH();
+}
+
+// y = op(A x) from the cell-block copy: all rows (row0 = false) or row 0 of
+// every cell (row0 = true, output index = cell).
+template <typename VT, typename XT, class Epi>
+void launch_bsr(cudaStream_t st, const deco_csr_s* A, int sw, bool row0, const XT* x, Epi epi) {
+  const int nbr = A->n / A->bbs;
+  if (nbr <= 0) return;
+  const VT* bv;
+  if constexpr (sizeof(VT) == 4) bv = A->bv32.get(); else bv = A->bv.get();
+  const long long plane = (long long)A->nblk * A->bbs;
+  if (A->bbs == 2) {
+    if (row0) launch_bsr_bs<2, true, VT, XT, Epi>(st, sw, nbr, A->br.get(), A->bc.get(), bv, plane, x, epi);
+    else launch_bsr_bs<2, false, VT, XT, Epi>(st, sw, nbr, A->br.get(), A->bc.get(), bv, plane, x, epi);
+  } else {
+    if (row0) launch_bsr_bs<3, true, VT, XT, Epi>(st, sw, nbr, A->br.get(), A->bc.get(), bv, plane, x, epi);
+    else launch_bsr_bs<3, false, VT, XT, Epi>(st, sw, nbr, A->br.get(), A->bc.get(), bv, plane, x, epi);
+  }
+}
+
 // heuristic width: about two vector loads per lane per row, the best width
 // measured on B200 for 7- and 14-entry rows in float64 (W = 2) and float32 (W = 4)
 inline int heuristic_subwarp(double avg_row, int W) {
@@ -139,10 +246,27 @@ inline int heuristic_subwarp(double avg_row, int W) {
 // float32 values: heuristic, refined by timing candidates when ctx->autotune.
 int tuned_subwarp(deco_ctx_s* ctx, deco_csr_s* A, bool f32);
 
-// y = op(A x) over rows 0, bs, 2bs, ... (nrows_out = n / bs rows)
+// Width for the cell-block kernel: about two blocks per lane, refined like
+// tuned_subwarp.
+int tuned_bsr_subwarp(deco_ctx_s* ctx, deco_csr_s* A, bool f32);
+
+// Builds (or rebuilds) the cell-block copy of A for bs x bs cells when the
+// zero padding stays within max_fill x nz stored values; otherwise A keeps no
+// block copy.  Float32 planes are made when A has float32 values.
+void make_bsr(deco_ctx_s* ctx, deco_csr_s* A, int bs, double max_fill = 1.25);
+void drop_bsr(deco_csr_s* A);
+
+// y = op(A x) over rows 0, bs, 2bs, ... (nrows_out = n / bs rows).  Uses the
+// cell-block copy when A has one, the product is over all rows or row 0 of
+// every cell, and x is aligned for the pair loads.
 template <typename VT, typename XT, class Epi>
 void spmv(deco_ctx_s* ctx, deco_csr_s* A, const XT* x, Epi epi, int bs = 1) {
   const bool f32 = sizeof(VT) == 4;
+  if (A->bbs > 1 && (bs == 1 || bs == A->bbs) && (!f32 || A->bv32) &&
+      (reinterpret_cast<uintptr_t>(x) % (A->bbs == 2 ? 2 * sizeof(XT) : sizeof(XT))) == 0) {
+    launch_bsr<VT, XT, Epi>(ctx->stream, A, tuned_bsr_subwarp(ctx, A, f32), bs != 1, x, epi);
+    return;
+  }
   const int sw = tuned_subwarp(ctx, A, f32);
   const VT* v;
   if constexpr (sizeof(VT) == 4) v = A->v32.get(); else v = A->v.get();

@@ -36,6 +36,9 @@ def lib():
         L.deco_gen_size.argtypes = [C.POINTER(GenParams), C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
         L.deco_gen_fill.argtypes = [C.POINTER(GenParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p]
+        L.deco_gen_fill_logk.argtypes = [C.POINTER(GenParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p]
+        L.deco_gen_grad_logk.argtypes = [C.POINTER(GenParams), C.c_void_p, C.c_void_p, C.c_void_p]
         L.deco_gen_uniform.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_longlong, C.c_void_p]
         L.deco_gen_uniform.restype = None
         _lib = L
@@ -85,6 +88,42 @@ def generate(p: GenParams, with_logk: bool = False) -> System:
     if rc != 0:
         raise ValueError(f"deco_gen_fill failed ({rc})")
     return System(n.value, r, c, v, b, p.bs, p, logk)
+
+
+def generate_from_logk(p: GenParams, logk: np.ndarray) -> System:
+    """The system of preset ``p`` with the permeability field ``exp(logk)`` (one value per cell)."""
+    n = C.c_int()
+    nnz = C.c_longlong()
+    if lib().deco_gen_size(C.byref(p), C.byref(n), C.byref(nnz)) != 0:
+        raise ValueError("deco_gen_size failed")
+    logk = np.ascontiguousarray(logk, np.float64)
+    if logk.size != p.nx * p.ny * p.nz:
+        raise ValueError("logk needs one value per cell")
+    r = np.empty(n.value + 1, np.int32)
+    c = np.empty(nnz.value, np.int32)
+    v = np.empty(nnz.value, np.float64)
+    b = np.empty(n.value, np.float64)
+    rc = lib().deco_gen_fill_logk(C.byref(p), logk.ctypes.data, r.ctypes.data, c.ctypes.data, v.ctypes.data,
+                                  b.ctypes.data)
+    if rc != 0:
+        raise ValueError(f"deco_gen_fill_logk failed ({rc})")
+    return System(n.value, r, c, v, b, p.bs, p, logk.copy())
+
+
+def grad_logk(p: GenParams, logk: np.ndarray | None, dLdA: np.ndarray) -> np.ndarray:
+    """dL/d ln k per cell from dL/dA given on the pattern of the system of ``p`` (chain rule through the
+    harmonic-mean transmissibilities)."""
+    dLdA = np.ascontiguousarray(dLdA, np.float64)
+    out = np.empty(p.nx * p.ny * p.nz, np.float64)
+    if logk is not None:
+        logk = np.ascontiguousarray(logk, np.float64)
+        if logk.size != out.size:
+            raise ValueError("logk needs one value per cell")
+    rc = lib().deco_gen_grad_logk(C.byref(p), logk.ctypes.data if logk is not None else None, dLdA.ctypes.data,
+                                  out.ctypes.data)
+    if rc != 0:
+        raise ValueError(f"deco_gen_grad_logk failed ({rc})")
+    return out
 
 
 def uniform(seed: int, stream: int, n: int) -> np.ndarray:

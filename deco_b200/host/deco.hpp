@@ -5,6 +5,7 @@
 //   FSAI<R,C,V>(ptree, A)              precond/FSAI/FSAI.hpp:14-47
 //   CPR<R,C,V,Mglobal,Mlocal>(ptree, A, b)   precond/CPR.hpp:42-172
 //   SOL<R,C,V>(ptree, A, precond, b, x)      solver/SOL.hpp:19-49
+//   ADJ<R,C,V>(ptree prec, A)                adjoint solve + dL/dA (no reference counterpart)
 //
 // A drop-in for the reference's call sequence (cpr.cpp:60-79):
 //   auto P = std::make_shared<CPR<int,int,double,FSAI,FSAI>>(param.get_child("prec"), A, b);
@@ -175,6 +176,54 @@ inline int weights_id(const std::string& w) {
   if (w == "quasiimpes_GE") return 2;
   throw std::invalid_argument("Unknown weights type " + w);
 }
+// the `prec` object of a parameter file (precond/CPR.hpp:49-65,118,130)
+inline deco_cpr_params cpr_params(const ptree& pt, int precision) {
+  deco_cpr_params prm{};
+  prm.block_size = pt.get<int>("block_size");
+  prm.pressure_id = pt.get<int>("pressure_id");
+  prm.seq = pt.get<int>("seq");
+  prm.weights = weights_id(pt.get<std::string>("weights"));
+  prm.use_drs = pt.get<int>("use_drs");
+  prm.drs_e_dd = pt.get<double>("drs.e_dd");
+  prm.drs_e_ps = pt.get<double>("drs.e_ps");
+  prm.cpd = pt.get<int>("CPD");
+  prm.tol_zero = pt.get<double>("tol_zero");
+  const std::string glo = pt.get<std::string>("prec_glo.type"), loc = pt.get<std::string>("prec_loc.type");
+  auto stage = [](const std::string& t) {
+    if (t == "FSAI") return 0;
+    if (t == "Jacobi") return 1;
+    throw gpu_error(DECO_ERR_UNSUPPORTED, "the GPU path builds FSAI or Jacobi stages (got " + t +
+                                              "); hypre AMG stays on the CPU build");
+  };
+  prm.glo_type = stage(glo);
+  prm.loc_type = stage(loc);
+  prm.glo_block_size = pt.get<int>("prec_glo.block_size", prm.block_size);
+  prm.loc_block_size = pt.get<int>("prec_loc.block_size", 1);
+  prm.glo_tol_rel = pt.get<double>("prec_glo.tol_rel", 0.0);
+  prm.glo_tol_abs = pt.get<double>("prec_glo.tol_abs", 0.0);
+  prm.glo_power = pt.get<int>("prec_glo.power", 1);
+  prm.loc_tol_rel = pt.get<double>("prec_loc.tol_rel");
+  prm.loc_tol_abs = pt.get<double>("prec_loc.tol_abs", 0.0);
+  prm.loc_power = pt.get<int>("prec_loc.power", 1);
+  prm.precision = pt.get<int>("precision", precision);
+  return prm;
+}
+
+// the `sol` object of a parameter file (solver/SOL.hpp:19-39, rgmres.tpp:13-16)
+inline deco_sol_params sol_params(const ptree& pt, int precision, bool use_x0) {
+  deco_sol_params sp{};
+  const std::string type = pt.get<std::string>("type");
+  if (type == "rgmres") sp.type = 0;
+  else if (type == "lgmres") sp.type = 1;
+  else throw std::invalid_argument("Invalid solver type: " + type);
+  sp.reltol = pt.get<double>("reltol");
+  sp.restart = pt.get<int>("restart");
+  sp.itmax = pt.get<int>("itmax");
+  sp.verbosity = pt.get<int>("verbosity", 0);
+  sp.precision = pt.get<int>("precision", precision);
+  sp.use_x0 = use_x0 ? 1 : 0;
+  return sp;
+}
 }  // namespace detail
 
 template <typename R = int, typename C = int, typename V = double,
@@ -189,27 +238,9 @@ class CPR : public CPRBase<V> {
 
   // precision: 64, or 32 for the float32 preconditioner (ptree key "precision" overrides)
   CPR(const ptree& pt, std::shared_ptr<CSR<R, C, V>> A_, V*& b, int precision = 64) : A(A_), param(pt) {
-    deco_cpr_params prm{};
-    prm.block_size = bs = pt.get<int>("block_size");
-    prm.pressure_id = p = pt.get<int>("pressure_id");
-    prm.seq = pt.get<int>("seq");
-    prm.weights = detail::weights_id(pt.get<std::string>("weights"));
-    prm.use_drs = pt.get<int>("use_drs");
-    prm.drs_e_dd = pt.get<double>("drs.e_dd");
-    prm.drs_e_ps = pt.get<double>("drs.e_ps");
-    prm.cpd = pt.get<int>("CPD");
-    prm.tol_zero = pt.get<double>("tol_zero");
-    const std::string glo = pt.get<std::string>("prec_glo.type"), loc = pt.get<std::string>("prec_loc.type");
-    if (glo != "FSAI" || loc != "FSAI")
-      throw gpu_error(DECO_ERR_UNSUPPORTED, "the GPU path builds FSAI for prec_glo and prec_loc (got " + glo + ", " +
-                                                loc + "); hypre AMG and Jacobi stay on the CPU build");
-    prm.glo_tol_rel = pt.get<double>("prec_glo.tol_rel");
-    prm.glo_tol_abs = pt.get<double>("prec_glo.tol_abs");
-    prm.glo_power = pt.get<int>("prec_glo.power");
-    prm.loc_tol_rel = pt.get<double>("prec_loc.tol_rel");
-    prm.loc_tol_abs = pt.get<double>("prec_loc.tol_abs", 0.0);
-    prm.loc_power = pt.get<int>("prec_loc.power", 1);
-    prm.precision = pt.get<int>("precision", precision);
+    deco_cpr_params prm = detail::cpr_params(pt, precision);
+    bs = prm.block_size;
+    p = prm.pressure_id;
     check(deco_cpr_create(context(), A->dev, b, &prm, &this->dev), "deco_cpr_create");
     deco_csr hp = nullptr;
     check(deco_cpr_pressure(this->dev, &hp), "deco_cpr_pressure");
@@ -271,17 +302,7 @@ class SOL {
  private:
   V* owned_x = nullptr;
   void run(deco_cpr P, int precision) {
-    deco_sol_params sp{};
-    const std::string type = param.get<std::string>("type");
-    if (type == "rgmres") sp.type = 0;
-    else if (type == "lgmres") sp.type = 1;
-    else throw std::invalid_argument("Invalid solver type: " + type);
-    sp.reltol = param.get<double>("reltol");
-    sp.restart = param.get<int>("restart");
-    sp.itmax = param.get<int>("itmax");
-    sp.verbosity = param.get<int>("verbosity", 0);
-    sp.precision = param.get<int>("precision", precision);
-    sp.use_x0 = x != nullptr;
+    deco_sol_params sp = detail::sol_params(param, precision, x != nullptr);
     if (!x) {
       if (cudaMalloc(&owned_x, sizeof(V) * A->n) != cudaSuccess) throw gpu_error(DECO_ERR_ALLOC, "cudaMalloc x");
       x = owned_x;
@@ -296,6 +317,56 @@ class SOL {
     time_ms = res.t_solve_ms;
     resvec.resize(iter);
   }
+};
+
+// Adjoint of the solve x = A^{-1} b (no counterpart in the reference).  For a
+// loss L(x) with g = dL/dx:  A^T lambda = g,  dL/db = lambda,
+// dL/dA_ij = -lambda_i x_j on A's pattern.  Built from A with its ORIGINAL
+// values (before a forward CPR decouples it in place): A^T is transposed on the
+// device and decoupled by its own CPR.  solve() takes any number of right-hand
+// sides; the forward x is the only state the gradient needs.
+template <typename R = int, typename C = int, typename V = double>
+class ADJ {
+ public:
+  const ptree& param;
+  deco_adjoint dev = nullptr;
+  C n = 0;
+  int iter = 0, flag = 1;
+  double res_abs = 0, res_rel = 0, time_ms = 0;
+  std::vector<double> resvec;
+
+  ADJ(const ptree& prec, std::shared_ptr<CSR<R, C, V>> A, int precision = 64) : param(prec), n(A->n) {
+    deco_cpr_params prm = detail::cpr_params(prec, precision);
+    precision_ = prm.precision;
+    check(deco_adjoint_create(context(), A->dev, &prm, &dev), "deco_adjoint_create");
+  }
+  ~ADJ() {
+    if (dev) deco_adjoint_destroy(dev);
+  }
+  ADJ(const ADJ&) = delete;
+  ADJ& operator=(const ADJ&) = delete;
+
+  // lambda = A^{-T} g (device pointers); lambda is the initial guess if use_x0
+  void solve(const ptree& sol, const V* g, V* lambda, bool use_x0 = false) {
+    deco_sol_params sp = detail::sol_params(sol, precision_, use_x0);
+    resvec.assign((size_t)sp.itmax + 1, 0.0);
+    deco_sol_result res{};
+    check(deco_adjoint_solve(context(), dev, g, lambda, &sp, &res, resvec.data()), "deco_adjoint_solve");
+    iter = res.iter;
+    flag = res.flag;
+    res_abs = res.res_abs;
+    res_rel = res.res_rel;
+    time_ms = res.t_solve_ms;
+    resvec.resize(iter);
+  }
+
+  // grad[e] = alpha * lambda_i * x_j over A's stored entries (dL/dA for alpha = -1)
+  static void grad_A(const CSR<R, C, V>& A, const V* lambda, const V* x, V* grad, V alpha = -1) {
+    check(deco_grad_A_pattern(context(), A.dev, lambda, x, alpha, grad), "deco_grad_A_pattern");
+  }
+
+ private:
+  int precision_ = 64;
 };
 
 }  // namespace deco

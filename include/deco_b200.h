@@ -82,6 +82,16 @@ int deco_csr_make_f32(deco_ctx ctx, deco_csr A);
 /* SpMV sub-warp width in use (1..32) and the one the autotuner picked. */
 int deco_csr_subwarp(deco_csr A, int* sw);
 int deco_csr_set_subwarp(deco_csr A, int sw);
+/* Cell-block copy for matrices made of bs x bs cell blocks (bs 2 or 3): one
+ * column index per block, entries the pattern lacks stored as zeros, values in
+ * row planes.  Every later product with A reads it (all rows, or row 0 of each
+ * cell for a restricted product with the same bs).  CPR setup adds it to its
+ * system and to the global FSAI factors.  Not built (status OK, *nblk = 0 from
+ * deco_csr_blocks) when padding would exceed a quarter of the stored entries;
+ * bs = 0 removes it.  No counterpart in the reference (core/CSR.hpp stores CSR
+ * only). */
+int deco_csr_set_blocks(deco_ctx ctx, deco_csr A, int bs);
+int deco_csr_blocks(deco_csr A, int* bs, int* nblk);
 
 /* y = A x (bs == 1), or the restricted product of alg::spmv with bs > 1:
  * y[i/bs] = (A x)[i] for rows i = 0, bs, 2bs, ...   (core/alg.hpp:50-64,
@@ -104,6 +114,9 @@ int deco_fsai_create(deco_ctx ctx, deco_csr A, double tol_rel, double tol_abs, i
                      deco_fsai* out);
 int deco_fsai_destroy(deco_fsai F);
 int deco_fsai_info(deco_fsai F, int* n, int* nz, int* max_order);
+/* Cell-block copies of the two factors (deco_csr_set_blocks): block size (0
+ * without) and stored blocks of FL and of FU^T. */
+int deco_fsai_blocks(deco_fsai F, int* bs, int* nblk_lower, int* nblk_upper);
 /* FL (lower, diagonal last) and FU^T (upper) in the reference's layout. */
 int deco_fsai_download(deco_ctx ctx, deco_fsai F, int* h_Lr, int* h_Lc, double* h_Lv, int* h_Ur, int* h_Uc,
                        double* h_Uv);
@@ -129,7 +142,7 @@ int deco_fsai_apply_static(deco_ctx ctx, deco_fsai F, const double* d_x, double*
 typedef struct deco_cpr_params {
   int block_size;        /* prec.block_size (2 or 3)                         */
   int pressure_id;       /* prec.pressure_id                                 */
-  int seq;               /* prec.seq: 0, 1 or 3                              */
+  int seq;               /* prec.seq: 0, 1, 2 or 3                           */
   int weights;           /* prec.weights: 0 none, 1 quasiimpes, 2 quasiimpes_GE */
   int use_drs;           /* prec.use_drs                                     */
   double drs_e_dd;       /* prec.drs.e_dd                                    */
@@ -140,11 +153,16 @@ typedef struct deco_cpr_params {
   double loc_tol_rel, loc_tol_abs; int loc_power;  /* prec.prec_loc.{tol_rel,tol_abs,power} */
   int precision;         /* 64: float64 preconditioner; 32: float32 factors,
                             float32 A copy and float32 vectors inside the apply */
+  int glo_type;          /* prec.prec_glo.type: 0 FSAI, 1 Jacobi (CPR<...,Jacobi,...>) */
+  int loc_type;          /* prec.prec_loc.type: 0 FSAI, 1 Jacobi                */
+  int glo_block_size;    /* prec.prec_glo.block_size: block size of the Jacobi of
+                            seq 2 or of a Jacobi global stage (1: point Jacobi) */
+  int loc_block_size;    /* prec.prec_loc.block_size (Jacobi local stage)       */
 } deco_cpr_params;
 
 int deco_cpr_create(deco_ctx ctx, deco_csr A, double* d_b, const deco_cpr_params* prm, deco_cpr* out);
 int deco_cpr_destroy(deco_cpr P);
-/* x = M^{-1} r with the configured sequence (apply_seq0/1/3, CPR.hpp:176-299). */
+/* x = M^{-1} r with the configured sequence (apply_seq0/1/2/3, CPR.hpp:176-299). */
 int deco_cpr_apply(deco_ctx ctx, deco_cpr P, const double* d_r, double* d_x);
 /* Borrowed handles of the pressure matrix and the two FSAI factors
  * (which = 0 global on A, 1 local on A_pp).  Valid while P lives. */
@@ -156,6 +174,13 @@ int deco_cpr_fsai(deco_cpr P, int which, deco_fsai* F);
 int deco_cpr_timings(deco_cpr P, double* h_ms5);
 /* Number of diagonal entries fix_diag replaced (CPR.hpp:753-840). */
 int deco_cpr_fixed_diagonals(deco_cpr P, int* count);
+/* Decouples another right-hand side d_b (n doubles, in place) with the row
+ * operations deco_cpr_create applied to A and its b: the same per-cell row
+ * swap, weights, DRS reset, IMPES sum and CPD product, rounded identically,
+ * so the result is bit-identical to a vector decoupled by deco_cpr_create.
+ * The reference decouples only the b it is constructed with
+ * (precond/CPR.hpp:42-172); this serves several right-hand sides per setup. */
+int deco_cpr_decouple_rhs(deco_ctx ctx, deco_cpr P, double* d_b);
 
 /* ------------------------------------------------------------------ solve
  * SOL<R,C,V>(ptree sol, A, precond, b, x) of solver/SOL.hpp:19-39 with
@@ -195,6 +220,41 @@ typedef struct deco_sol_result {
  * (rgmres.tpp:61) but discards. */
 int deco_gmres_solve(deco_ctx ctx, deco_csr A, deco_cpr P, const double* d_b, double* d_x,
                      const deco_sol_params* prm, deco_sol_result* res, double* h_resvec);
+
+/* ---------------------------------------------------------------- adjoint
+ * Differentiation of x = A^{-1} b (no counterpart in the reference).  For a
+ * loss L(x) with g = dL/dx the adjoint solve is A^T lambda = g; then
+ * dL/db = lambda and dL/dA_ij = -lambda_i x_j on A's sparsity pattern.  The
+ * adjoint system is A^T transposed first and then decoupled per cell by the
+ * same CPR setup as the forward system (decoupling the transpose of an
+ * already decoupled matrix leaves singular cell blocks), so lambda solves
+ * the original A^T lambda = g, with no back-transformation.  Only x from the
+ * forward solve is kept; no Krylov basis is stored. */
+
+/* At = A^T on the device: rows of At list their entries in ascending column
+ * order (the order of core/CSR.hpp:193-206's sequential scatter). */
+int deco_csr_transpose(deco_ctx ctx, deco_csr A, deco_csr* At);
+
+/* d_grad[e] = alpha * (d_lambda[i] * d_x[j]) for every stored entry e = (i, j)
+ * of A, in A's CSR order; alpha = -1 gives dL/dA. */
+int deco_grad_A_pattern(deco_ctx ctx, deco_csr A, const double* d_lambda, const double* d_x, double alpha,
+                        double* d_grad);
+
+typedef struct deco_adjoint_s* deco_adjoint;
+
+/* Builds A^T from A (its current values: pass the matrix before any forward
+ * decoupling) and the CPR preconditioner of the transposed system.  A is not
+ * modified and may be destroyed afterwards. */
+int deco_adjoint_create(deco_ctx ctx, deco_csr A, const deco_cpr_params* prm, deco_adjoint* out);
+int deco_adjoint_destroy(deco_adjoint J);
+/* Solves A^T d_lambda = d_g (d_g is not modified); prm, res, h_resvec as in
+ * deco_gmres_solve.  Any number of right-hand sides may be solved with one
+ * deco_adjoint. */
+int deco_adjoint_solve(deco_ctx ctx, deco_adjoint J, const double* d_g, double* d_lambda,
+                       const deco_sol_params* prm, deco_sol_result* res, double* h_resvec);
+/* The transposed matrix (decoupled in place by the adjoint's CPR) and its
+ * preconditioner, owned by J. */
+int deco_adjoint_parts(deco_adjoint J, deco_csr* At, deco_cpr* P);
 
 #ifdef __cplusplus
 }

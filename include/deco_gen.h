@@ -58,6 +58,17 @@ int deco_gen_size(const deco_gen_params* p, int* n, long long* nnz);
 int deco_gen_fill(const deco_gen_params* p, int* r, int* c, double* v, double* b,
                   double* logk);
 
+/* The same system assembled from a caller-given ln(k) field (nx*ny*nz values)
+ * instead of the seeded one; b is the seeded right-hand side as before. */
+int deco_gen_fill_logk(const deco_gen_params* p, const double* logk, int* r, int* c, double* v, double* b);
+
+/* Chain rule from the matrix to the permeability: given dL/dA on the pattern
+ * (nnz values, in the order deco_gen_fill writes them), writes dL/d ln k for
+ * every cell.  Every transmissibility-dependent entry is T times a coefficient
+ * independent of k, with T = 2 k_a k_b / (k_a + k_b) * mult per face; wells and
+ * accumulation terms do not depend on k.  logk == NULL uses the seeded field. */
+int deco_gen_grad_logk(const deco_gen_params* p, const double* logk, const double* dLdA, double* dLdlogk);
+
 /* Uniform [0,1) vector from the same counter-based generator (stream id lets
  * callers draw independent right-hand sides). */
 void deco_gen_uniform(unsigned long long seed, unsigned long long stream, long long n,

@@ -38,6 +38,10 @@ def lib():
     if _lib is None:
         if not os.path.exists(LIB):
             build()
+        # OpenBLAS (pthreads build) must not start its own threads inside the
+        # reference's OpenMP loops (FSAI local solves call LAPACKE per row):
+        # single-threaded BLAS, and no per-call "OpenMP loop" warning
+        os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
         L = C.CDLL(LIB)
         vp, ip, dp = C.c_void_p, C.c_void_p, C.c_void_p
         L.ref_spmv.argtypes = [C.c_int, ip, ip, dp, dp, dp, C.c_int]

@@ -55,6 +55,8 @@ MPI_Comm deco_comm = MPI_COMM_WORLD;
 using Mat = CSR<int, int, double>;
 using CPRff = CPR<int, int, double, FSAI, FSAI>;
 using CPRjf = CPR<int, int, double, Jacobi, FSAI>;
+using CPRfj = CPR<int, int, double, FSAI, Jacobi>;
+using CPRjj = CPR<int, int, double, Jacobi, Jacobi>;
 
 namespace {
 
@@ -151,8 +153,18 @@ void* ref_cpr_create(const char* params_json, int n, const int* r, const int* c,
   std::memcpy(h->b, b, sizeof(double) * n);
   const auto& prec = h->pt.get_child("prec");
   std::string glo = prec.get<std::string>("prec_glo.type");
+  std::string loc = prec.get<std::string>("prec_loc.type");
   double t0 = now();
-  if (glo == "Jacobi") {
+  if (glo == "Jacobi" && loc == "Jacobi") {
+    auto P = std::make_shared<CPRjj>(prec, h->A, h->b);
+    h->Ap = P->Ap;
+    h->P = P;
+  } else if (loc == "Jacobi") {
+    auto P = std::make_shared<CPRfj>(prec, h->A, h->b);
+    h->Ap = P->Ap;
+    h->Fglo = P->Fglo.get();
+    h->P = P;
+  } else if (glo == "Jacobi") {
     auto P = std::make_shared<CPRjf>(prec, h->A, h->b);
     h->Ap = P->Ap;
     h->Floc = P->Floc.get();

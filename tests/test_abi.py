@@ -91,3 +91,12 @@ def test_params_mapping_follows_reference_keys():
     assert (sp.type, sp.restart, sp.itmax, sp.verbosity) == (1, 30, 100, 1) and sp.reltol == 1e-6
     with pytest.raises(d.DecoError):
         d.sol_params({"type": "pcg", "reltol": "1", "restart": "1", "itmax": "1"})
+
+
+def test_handles_hold_no_reference_cycles():
+    """Borrowed views (the pressure matrix, the FSAI factors) point at their owner,
+    never the other way, so dropping a CPR frees it by reference counting alone."""
+    import inspect
+    import deco_b200
+    src = inspect.getsource(deco_b200.CPR.__init__)
+    assert "self.Ap" not in src and "_owner = self" not in src

@@ -75,3 +75,32 @@ def test_driver_rejects_cpu_only_preconditioners(tmp_path):
     param = write_params(tmp_path, {"format": "synthetic", "preset": "1"}, prec, sol_json())
     rc, it, res, out = run(param)
     assert rc == 3 and "hypre" in out.stderr
+
+
+@pytest.mark.gpu
+def test_driver_adjoint_section(tmp_path):
+    """The optional "adjoint" object: A^T lambda = dL/dx for L = sum_k w_k p(cell_k),
+    with CPR on A^T, against the oracle's adjoint of the same seeded observations."""
+    from deco_b200 import gen
+    from oracle import adjoint
+    prec, sol = cpr_json(2), sol_json(reltol=1e-10)
+    io = {"format": "synthetic", "preset": "1", "seed": "1234"}
+    text = json.dumps({"IO": io, "sol": sol, "prec": prec, "parallel": {"hardware": "GPU"},
+                       "adjoint": {"observations": "12", "seed": "5",
+                                   "wfile_lambda": str(tmp_path / "lambda.bin")}})
+    param = tmp_path / "param.json"
+    param.write_text(text)
+    rc, it, res, out = run(str(param))
+    assert rc == 0, out.stderr + out.stdout
+    assert re.search(r"adjoint iteration count =\s+\d+", out.stdout)
+    s = gen.generate(gen.preset(1, 1234))
+    ncell = s.n // 2
+    u = gen.uniform(5, 77, 24)
+    g = np.zeros(s.n)
+    for k in range(12):
+        g[min(ncell - 1, int(u[2 * k] * ncell)) * 2] += u[2 * k + 1]
+    raw = np.fromfile(tmp_path / "lambda.bin", dtype=np.uint8)
+    assert int(np.frombuffer(raw[:4].tobytes(), np.int32)[0]) == s.n
+    lam = np.frombuffer(raw[4:].tobytes(), np.float64)
+    lam_ref = adjoint.adjoint(prec, sol, s.r, s.c, s.v, g, "port")["x"]
+    assert np.linalg.norm(lam - lam_ref) / np.linalg.norm(lam_ref) < 1e-7

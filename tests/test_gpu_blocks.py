@@ -1,0 +1,107 @@
+"""The cell-block (one index per bs x bs block) products against the CPU oracle.
+
+Bars: float64 products within 1e-12 relative of the oracle's SpMV (core/alg.hpp:50-64)
+for all rows and for the restricted product over row 0 of every cell; float32 values
+within 1e-6; padding with explicit zeros leaves the product unchanged; CPR apply and
+the solve through block copies keep the CPR parity bars.
+"""
+import numpy as np
+import pytest
+
+from conftest import cpr_json, rel, sol_json
+from deco_b200 import gen
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def d():
+    import deco_b200
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    deco_b200.default_context()
+    return deco_b200
+
+
+def cuda(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+SYSTEMS = {
+    "c1_bs2": lambda: gen.generate(gen.preset(1)),
+    "bs3_faults": lambda: gen.grid(12, 10, 6, bs=3, fault_frac=0.02, layered=1, sigma=2.0),
+    "bs2_small": lambda: gen.grid(5, 4, 3, bs=2, seed=7),
+}
+
+
+@pytest.mark.parametrize("name", list(SYSTEMS))
+def test_block_products_match_oracle(d, name):
+    from oracle import port
+    s = SYSTEMS[name]()
+    A = d.CSR.from_system(s)
+    A.set_blocks(s.bs)
+    bs, nblk = A.blocks
+    assert bs == s.bs and nblk * bs * bs == s.nnz  # generated systems are dense cell blocks
+    x = np.random.default_rng(0).standard_normal(s.n)
+    assert rel(A.apply(cuda(x)).cpu().numpy(), port.spmv(s.r, s.c, s.v, x)) < 1e-12
+    assert rel(A.apply(cuda(x), bs=s.bs).cpu().numpy(), port.spmv(s.r, s.c, s.v, x, s.bs)) < 1e-12
+    y32 = A.apply_f32(cuda(x.astype(np.float32))).cpu().numpy()
+    v32 = s.v.astype(np.float32).astype(np.float64)
+    assert rel(y32, port.spmv(s.r, s.c, v32, x.astype(np.float32).astype(np.float64))) < 1e-6
+    # a pointer not aligned for the pair loads takes the scalar path, same result
+    xx = cuda(np.concatenate([[0.0], x]))
+    assert rel(A.apply(xx[1:]).cpu().numpy(), port.spmv(s.r, s.c, s.v, x)) < 1e-12
+    A.set_blocks(0)
+    assert A.blocks == (0, 0)
+
+
+def test_padding_with_zeros(d):
+    """Entries missing from a cell block (a filtered pattern) are stored as zeros."""
+    from oracle import port
+    s = gen.grid(9, 8, 5, bs=2, seed=3)
+    keep = np.ones(s.nnz, bool)
+    rows = np.repeat(np.arange(s.n), np.diff(s.r))
+    drop = (rows % 2 == 0) & (s.c % 2 == 1) & (s.c // 2 != rows // 2)  # p rows lose their s columns off the diagonal
+    drop &= np.random.default_rng(1).random(s.nnz) < 0.3
+    keep &= ~drop
+    c, v = s.c[keep], s.v[keep]
+    r = np.zeros(s.n + 1, np.int32)
+    np.cumsum(np.bincount(rows[keep], minlength=s.n), out=r[1:])
+    A = d.CSR(s.n, s.n, r, c, v)
+    A.set_blocks(2)
+    bs, nblk = A.blocks
+    assert bs == 2 and nblk * 4 > len(c)
+    x = np.random.default_rng(2).standard_normal(s.n)
+    assert rel(A.apply(cuda(x)).cpu().numpy(), port.spmv(r, c, v, x)) < 1e-12
+
+
+def test_too_much_padding_keeps_csr(d):
+    """A scalar (diagonal-only) matrix would be 4x padded: no block copy is made."""
+    n = 1000
+    r = np.arange(n + 1, dtype=np.int32)
+    c = np.arange(n, dtype=np.int32)
+    A = d.CSR(n, n, r, c, np.ones(n))
+    A.set_blocks(2)
+    assert A.blocks == (0, 0)
+    assert rel(A.apply(cuda(np.arange(n, dtype=np.float64))).cpu().numpy(), np.arange(n, dtype=np.float64)) == 0
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_cpr_builds_blocks_and_keeps_parity(d, precision):
+    from oracle import port
+    s = gen.generate(gen.preset(1))
+    prec = cpr_json(2)
+    A = d.CSR.from_system(s)
+    b = cuda(s.b)
+    P = d.CPR(prec, A, b, precision)
+    assert A.blocks[0] == 2
+    assert P.fsai(0).n == s.n
+    O = port.Cpr(prec, s.r, s.c, s.v, s.b)
+    rvec = np.random.default_rng(5).standard_normal(s.n)
+    tol = 1e-12 if precision == 64 else 1e-5
+    assert rel(P.apply(cuda(rvec)).cpu().numpy(), O.apply(rvec)) < tol
+    S = d.SOL(sol_json(), A, P, b, precision=precision)
+    ref_it = O.solve(sol_json())["iter"]
+    assert S.flag == 0 and abs(S.iter - ref_it) <= max(2, 0.1 * ref_it)
