@@ -30,6 +30,7 @@ With --gpus N > 1 (torchrun) every rank solves its own copy of the system
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -161,6 +162,108 @@ def run_reference(args, rank, world):
     }))
 
 
+def bench_batch(args):
+    """64 independent two-phase systems (cells log-uniform in 10k-500k), 8
+    right-hand sides each, one lockstep CPR-GMRES solve per precision."""
+    import torch
+    import deco_b200 as d
+    from deco_b200 import gen
+    ctx = d.Context(0)
+    st = ctx.torch_stream
+    torch.cuda.set_stream(st)
+    r, c, v, ro, B, shapes = gen.batch(64, SEED, 10_000, 500_000, 2, 8)
+    n, nnz = int(ro[-1]), len(c)
+    dev = lambda a: torch.from_numpy(a).cuda()
+    r_d, c_d, v_d, B_d = dev(r), dev(c), dev(v), dev(B)
+    out = {}
+    for bits in (32, 64):
+        rows = []
+        for k in range(args.warmup + args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            A = d.CSR(n, n, r_d, c_d, v_d, ctx)
+            Bt = d.Batch(PREC, A, ro, 8, precision=bits)
+            X = Bt.solve(SOL, B_d)
+            e1.record(st)
+            e1.synchronize()
+            if k >= args.warmup:
+                rows.append((e0.elapsed_time(e1), Bt.result, Bt.iters.copy(), Bt.res_rel.copy(), Bt.widths.copy()))
+            del Bt, A, X
+        ms = statistics.mean(t[0] for t in rows)
+        res, it, rr, w = rows[-1][1], rows[-1][2], rows[-1][3], rows[-1][4]
+        out["mixed" if bits == 32 else "fp64"] = {
+            "time_s": ms / 1e3, "solve_ms": res["t_solve_ms"], "cycles": res["cycles"], "graph": res["graph"],
+            "converged": res["converged"], "instances": int(it.size), "iterations_max": int(it.max()),
+            "iterations_median": float(statistics.median(it.ravel().tolist())),
+            "max_true_rel_residual": float(rr.max()), "widths": sorted(set(int(x) for x in w)),
+            "instances_per_s": it.size / (ms / 1e3)}
+    line = {"metric": "batched CPR-GMRES time-to-1e-8 (64 systems x 8 right-hand sides)",
+            "value": out["mixed"]["time_s"], "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": False, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": f"config 4: 64 two-phase systems, cells log-uniform 10k-500k ({n // 2} cells, "
+                                   f"{n} rows, {nnz} nnz), 8 uniform right-hand sides each; CPR seq 3 + GMRES(50)",
+                       "seed": SEED}, **out,
+            "speedup_mixed_vs_fp64": out["fp64"]["time_s"] / out["mixed"]["time_s"]}
+    print(json.dumps(line))
+
+
+def bench_adjoint(args):
+    """64x64x32 log-permeability system: forward CPR-GMRES, adjoint CPR-GMRES on A^T
+    and the on-pattern gradient, float64 and mixed."""
+    import numpy as np
+    import torch
+    import deco_b200 as d
+    from deco_b200 import gen
+    ctx = d.Context(0)
+    st = ctx.torch_stream
+    torch.cuda.set_stream(st)
+    p = gen.preset(5, SEED)
+    s = gen.generate(p, with_logk=True)
+    rng = np.random.default_rng(2024)
+    obs = rng.choice(s.n // 2, 20, replace=False)
+    g = np.zeros(s.n)
+    g[2 * obs] = rng.random(20)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    r_d, c_d, v_d, b_d, g_d = dev(s.r), dev(s.c), dev(s.v), dev(s.b), dev(g)
+    out = {}
+    for bits in (64, 32):
+        rows = []
+        for k in range(args.warmup + args.steps):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            ev[0].record(st)
+            A = d.CSR(s.n, s.n, r_d, c_d, v_d, ctx)
+            b = b_d.clone()
+            P = d.CPR(PREC, A, b, bits)
+            S = d.SOL(SOL, A, P, b, precision=bits)
+            ev[1].record(st)
+            A0 = d.CSR(s.n, s.n, r_d, c_d, v_d, ctx)
+            J = d.ADJ(PREC, A0, bits)
+            lam = J.solve(SOL, g_d)
+            ev[2].record(st)
+            grad = A0.grad_pattern(lam, S.x)
+            ev[3].record(st)
+            ev[3].synchronize()
+            if k >= args.warmup:
+                rows.append((ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2]), ev[2].elapsed_time(ev[3]),
+                             S.iter, J.iter))
+            del S, P, A, J, A0, lam, grad
+        f = statistics.mean(t[0] for t in rows)
+        a = statistics.mean(t[1] for t in rows)
+        gk = statistics.mean(t[2] for t in rows)
+        alg = 12 * s.nnz + 8 * (s.n + 1) + 8 * s.n
+        out["fp64" if bits == 64 else "mixed"] = {
+            "forward_ms": f, "adjoint_ms": a, "adjoint_over_forward": a / f, "grad_kernel_ms": gk,
+            "grad_kernel_gbs": alg / gk / 1e6, "forward_iterations": rows[-1][3], "adjoint_iterations": rows[-1][4]}
+    print(json.dumps({"metric": "adjoint gradient time (forward + transpose CPR-GMRES + dL/dA on pattern)",
+                      "value": (out["fp64"]["forward_ms"] + out["fp64"]["adjoint_ms"] + out["fp64"]["grad_kernel_ms"])
+                      / 1e3, "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                      "higher_is_better": False, "dtype": "f64", "data": "synthetic",
+                      "config": {"workload": "config 5: 64x64x32 two-phase grid from a seeded log-permeability "
+                                             "field, bs 2, 262,144 rows; L = weighted pressures at 20 seeded cells; "
+                                             "CPR seq 3 + GMRES(50) to 1e-8 forward and adjoint", "seed": SEED},
+                      **out}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -173,7 +276,13 @@ def main():
     ap.add_argument("--kernels-only", action="store_true",
                     help="only the per-kernel timings (for profiler captures on a smaller --config)")
     ap.add_argument("--config", type=int, default=3, help="system preset (3 = the benchmark workload)")
+    ap.add_argument("--workload", default="solve", choices=["solve", "batch", "adjoint"],
+                    help="solve: the headline single-system solve; batch: config 4; adjoint: config 5")
     args = ap.parse_args()
+    if args.workload == "batch":
+        return bench_batch(args)
+    if args.workload == "adjoint":
+        return bench_adjoint(args)
     global CONFIG
     CONFIG = args.config
     rank = int(os.environ.get("RANK", 0))
@@ -239,10 +348,16 @@ def main():
     def timed(bits, k, host=False):
         if k == 0:
             return 0.0, [dict(ms=0, iter=0, flag=-1, res_rel=0, true_rel=0, setup_ms=0, solve_ms=0)], 0.0, 0
+        # no Python garbage-collection pause inside the timed steps (timeit's practice)
+        gc.collect()
+        gc.disable()
         barrier()
         l0 = lib().deco_launch_count()
         t0 = time.perf_counter()
-        infos = [step(bits, host) for _ in range(k)]
+        try:
+            infos = [step(bits, host) for _ in range(k)]
+        finally:
+            gc.enable()
         barrier()
         wall = time.perf_counter() - t0
         launches = lib().deco_launch_count() - l0

@@ -10,6 +10,7 @@ tensors; the native library does all the work.
   SOL   solver/SOL.hpp          SOL(sol, A, precond, b, x=None) solves in the constructor
   ADJ   (no reference counterpart) adjoint of the solve: A^T lambda = g with CPR on A^T;
         deco_b200.adjoint wraps forward + adjoint as a torch.autograd.Function
+  Batch (no reference counterpart) many systems x several right-hand sides in one lockstep solve
 
 Parameter dictionaries use the reference's JSON keys (values may be strings, as
 in the shipped param_*.json files).
@@ -21,9 +22,9 @@ import json
 
 import numpy as np
 
-from ._lib import CprParams, DecoError, SolParams, SolResult, check, lib
+from ._lib import BatchResult, CprParams, DecoError, SolParams, SolResult, check, lib
 
-__all__ = ["Context", "CSR", "FSAI", "CPR", "SOL", "ADJ", "DecoError", "default_context", "load_params",
+__all__ = ["Context", "CSR", "FSAI", "CPR", "SOL", "ADJ", "Batch", "DecoError", "default_context", "load_params",
            "cpr_params", "sol_params"]
 
 _WEIGHTS = {"none": 0, "quasiimpes": 1, "quasiimpes_GE": 2}
@@ -67,6 +68,10 @@ class Context:
 
     def set_autotune(self, on: bool):
         check(lib().deco_ctx_set_autotune(self.h, int(on)))
+
+    def trim(self):
+        """Returns the library's cached device blocks to the device memory pool."""
+        check(lib().deco_ctx_trim(self.h))
 
     def __del__(self):
         try:
@@ -477,4 +482,68 @@ class ADJ:
     def __del__(self):
         if getattr(self, "h", None):
             lib().deco_adjoint_destroy(self.h)
+            self.h = None
+
+
+class Batch:
+    """Independent systems, each with `nrhs` right-hand sides, solved together (no
+    counterpart in the reference).  A: the block-diagonal matrix of all systems
+    (decoupled in place, as CPR does); row_off: nsys + 1 cell-aligned row offsets.
+    Right-hand sides and solutions are row-interleaved: B[row * nrhs + k]."""
+
+    def __init__(self, prec: dict, A: CSR, row_off, nrhs: int, precision: int = 64):
+        self.ctx, self.A, self.n = A.ctx, A, A.n
+        self.row_off = np.ascontiguousarray(row_off, np.int32)
+        self.nsys, self.nrhs = len(self.row_off) - 1, int(nrhs)
+        self.params = cpr_params(prec, precision)
+        h = C.c_void_p()
+        check(lib().deco_batch_create(self.ctx.h, A.h, self.nsys, self.row_off.ctypes.data, self.nrhs,
+                                      C.byref(self.params), C.byref(h)))
+        self.h = h
+
+    @property
+    def widths(self) -> np.ndarray:
+        w = np.zeros(self.nsys, np.int32)
+        check(lib().deco_batch_info(self.h, None, None, None, w.ctypes.data))
+        return w
+
+    def apply(self, R, X=None):
+        """X = M^{-1} R for every column (the batch's CPR; row-interleaved multi-vectors)."""
+        torch = _torch()
+        R = _dev(R, torch.float64)
+        if X is None:
+            X = torch.empty(self.n * self.nrhs, dtype=torch.float64, device="cuda")
+        check(lib().deco_batch_apply(self.ctx.h, self.h, _ptr(R), _ptr(X)))
+        return X
+
+    def cpr(self):
+        """The batch's CPR (a borrowed handle; single-vector apply on the whole block-diagonal system)."""
+        h = C.c_void_p()
+        check(lib().deco_batch_cpr(self.h, C.byref(h)))
+        return h
+
+    def solve(self, sol: dict, B, X=None):
+        """X (CUDA float64, n * nrhs) solving every system for every column of B."""
+        torch = _torch()
+        B = _dev(B, torch.float64)
+        if X is None:
+            X = torch.empty(self.n * self.nrhs, dtype=torch.float64, device="cuda")
+        sp = sol_params(sol, self.params.precision)
+        q = self.nsys * self.nrhs
+        it = np.zeros(q, np.int32)
+        rr = np.zeros(q, np.float64)
+        fl = np.zeros(q, np.int32)
+        res = BatchResult()
+        check(lib().deco_batch_solve(self.ctx.h, self.h, _ptr(B), _ptr(X), C.byref(sp), it.ctypes.data,
+                                     rr.ctypes.data, fl.ctypes.data, C.byref(res)))
+        self.iters = it.reshape(self.nsys, self.nrhs)
+        self.res_rel = rr.reshape(self.nsys, self.nrhs)
+        self.flags = fl.reshape(self.nsys, self.nrhs)
+        self.result = {"max_iter": res.max_iter, "converged": res.converged, "cycles": res.cycles,
+                       "graph": bool(res.graph), "t_solve_ms": res.t_solve_ms}
+        return X
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().deco_batch_destroy(self.h)
             self.h = None

@@ -37,6 +37,11 @@ class SolResult(C.Structure):
                 ("t_matvec_ms", C.c_double), ("t_ortho_ms", C.c_double)]
 
 
+class BatchResult(C.Structure):
+    _fields_ = [("max_iter", C.c_int), ("converged", C.c_int), ("cycles", C.c_int), ("graph", C.c_int),
+                ("t_solve_ms", C.c_double)]
+
+
 # name -> (argtypes, restype); every function in include/deco_b200.h
 SIGNATURES = {
     "deco_last_error": ([], C.c_char_p),
@@ -47,6 +52,7 @@ SIGNATURES = {
     "deco_ctx_sync": ([vp], C.c_int),
     "deco_ctx_stream": ([vp, C.POINTER(vp)], C.c_int),
     "deco_ctx_set_autotune": ([vp, C.c_int], C.c_int),
+    "deco_ctx_trim": ([vp], C.c_int),
     "deco_csr_create": ([vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, C.c_int, C.POINTER(vp)], C.c_int),
     "deco_csr_destroy": ([vp], C.c_int),
     "deco_csr_info": ([vp, ip, ip, ip], C.c_int),
@@ -82,6 +88,12 @@ SIGNATURES = {
     "deco_adjoint_destroy": ([vp], C.c_int),
     "deco_adjoint_solve": ([vp, vp, vp, vp, C.POINTER(SolParams), C.POINTER(SolResult), vp], C.c_int),
     "deco_adjoint_parts": ([vp, C.POINTER(vp), C.POINTER(vp)], C.c_int),
+    "deco_batch_create": ([vp, vp, C.c_int, vp, C.c_int, C.POINTER(CprParams), C.POINTER(vp)], C.c_int),
+    "deco_batch_destroy": ([vp], C.c_int),
+    "deco_batch_info": ([vp, ip, ip, ip, vp], C.c_int),
+    "deco_batch_cpr": ([vp, C.POINTER(vp)], C.c_int),
+    "deco_batch_apply": ([vp, vp, vp, vp], C.c_int),
+    "deco_batch_solve": ([vp, vp, vp, vp, C.POINTER(SolParams), vp, vp, vp, C.POINTER(BatchResult)], C.c_int),
 }
 
 _lib = None

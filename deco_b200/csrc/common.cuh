@@ -63,9 +63,27 @@ int guard(F&& f) {
   }
 }
 
+// DECO_TRACE=1 diagnostics for host calls that take unusually long
+double trace_clock_ms();
+void trace_slow_call(const char* what, size_t bytes, double t0_ms);
+
 // Elements of slack after every device array: vectorised loads (16 bytes) may
 // touch up to 3 elements past the last valid one; the slack is zero-filled.
 constexpr size_t kPad = 16;
+
+// Device memory of the library.  Large blocks (>= 1 MiB) freed on a stream are
+// kept in a per-stream cache and handed to later requests on the SAME stream
+// (stream order makes the reuse safe), because the stream-ordered pool's
+// cudaMallocAsync occasionally stalls for hundreds of milliseconds on large
+// requests even when its reserved memory could serve them; a solve that
+// rebuilds its setup every step then allocates nothing after the first step.
+// Smaller blocks go straight to the pool.  DECO_CACHE=0 disables the cache;
+// deco_ctx_trim returns a stream's cached blocks to the pool.
+void* dev_alloc(size_t bytes, cudaStream_t s, size_t* capacity);
+void dev_free(void* p, size_t capacity, cudaStream_t s);
+void cache_attach_stream(cudaStream_t s);
+void cache_detach_stream(cudaStream_t s);  // frees the stream's cached blocks
+void cache_trim_stream(cudaStream_t s);
 
 // Owning device buffer with zeroed padding; moves, does not copy.
 template <typename T>
@@ -75,36 +93,33 @@ class DevBuf {
   explicit DevBuf(size_t n, cudaStream_t s = 0) { alloc(n, s); }
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_), s_(o.s_) { o.p_ = nullptr; o.n_ = 0; }
+  DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_), cap_(o.cap_), s_(o.s_) { o.p_ = nullptr; o.n_ = 0; o.cap_ = 0; }
   DevBuf& operator=(DevBuf&& o) noexcept {
-    if (this != &o) { release(); p_ = o.p_; n_ = o.n_; s_ = o.s_; o.p_ = nullptr; o.n_ = 0; }
+    if (this != &o) {
+      release();
+      p_ = o.p_; n_ = o.n_; cap_ = o.cap_; s_ = o.s_;
+      o.p_ = nullptr; o.n_ = 0; o.cap_ = 0;
+    }
     return *this;
   }
   ~DevBuf() { release(); }
 
-  // Stream-ordered allocation from the device's memory pool: no device-wide
-  // synchronisation, and freed blocks are reused by later allocations.
+  // Stream-ordered allocation (dev_alloc): no device-wide synchronisation.
   void alloc(size_t n, cudaStream_t s = 0) {
     release();
     n_ = n;
     s_ = s;
-    void* p = nullptr;
-    cudaError_t e = cudaMallocAsync(&p, (n + kPad) * sizeof(T), s);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      throw Error(DECO_ERR_ALLOC, "device allocation of " + std::to_string((n + kPad) * sizeof(T)) +
-                                      " bytes failed: " + cudaGetErrorString(e));
-    }
-    p_ = static_cast<T*>(p);
+    p_ = static_cast<T*>(dev_alloc((n + kPad) * sizeof(T), s, &cap_));
     DECO_CUDA(cudaMemsetAsync(p_ + n, 0, kPad * sizeof(T), s));
   }
   void zero(cudaStream_t s) {
     if (p_) DECO_CUDA(cudaMemsetAsync(p_, 0, (n_ + kPad) * sizeof(T), s));
   }
   void release() {
-    if (p_) cudaFreeAsync(p_, s_);
+    if (p_) dev_free(p_, cap_, s_);
     p_ = nullptr;
     n_ = 0;
+    cap_ = 0;
   }
   T* get() const { return p_; }
   size_t size() const { return n_; }
@@ -113,6 +128,7 @@ class DevBuf {
  private:
   T* p_ = nullptr;
   size_t n_ = 0;
+  size_t cap_ = 0;
   cudaStream_t s_ = 0;
 };
 
@@ -127,6 +143,8 @@ struct deco_ctx_s {
   int num_sms = 148;
   int autotune = 1;
   int bsr = 1;        // cell-block copies for CPR systems (DECO_BSR=0 disables)
+  int trace = 0;      // DECO_TRACE=1: host wall time of setup sub-steps on stderr
+  double trace_t = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // small pinned host buffer for scalar read-backs
   double* host_scalars = nullptr;
@@ -158,6 +176,10 @@ __host__ __device__ __forceinline__ long long cdiv(long long a, long long b) { r
 // exclusive scan of int counts[0..n) into out[0..n] (out[n] = total);
 // returns the total.  64-bit accumulation; throws if the total exceeds int32.
 long long exclusive_scan_int(deco_ctx_s* ctx, const int* counts, int* out, long long n);
+
+// DECO_TRACE=1: synchronises the stream and prints the wall time since the last
+// mark (setup diagnostics; no effect otherwise)
+void trace_mark(deco_ctx_s* ctx, const char* label);
 
 // grid size for a grid-stride kernel: a multiple of the SM count
 inline int grid_for(const deco_ctx_s* ctx, long long work, int block, int per_sm = 8) {

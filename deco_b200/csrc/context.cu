@@ -1,5 +1,8 @@
 // context.cu — error state, context lifecycle and the device exclusive scan
 // used by every count/compact step (filters, pattern extraction, transposes).
+#include <map>
+#include <mutex>
+#include <chrono>
 #include <atomic>
 #include <cstdlib>
 
@@ -12,6 +15,129 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 static std::atomic<long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+// ------------------------------------------------------------ block cache
+namespace {
+std::mutex g_cache_mu;
+std::map<cudaStream_t, std::multimap<size_t, void*>> g_cache;  // stream -> (capacity -> block)
+std::map<cudaStream_t, int> g_live;                            // streams of live contexts
+constexpr size_t kCacheMin = size_t(1) << 20;
+
+bool cache_on() {
+  static const bool on = [] {
+    const char* e = std::getenv("DECO_CACHE");
+    return !(e && std::atoi(e) == 0);
+  }();
+  return on;
+}
+}  // namespace
+
+void* dev_alloc(size_t bytes, cudaStream_t s, size_t* capacity) {
+  if (cache_on() && bytes >= kCacheMin) {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    auto it = g_cache.find(s);
+    if (it != g_cache.end()) {
+      auto& mm = it->second;
+      auto b = mm.lower_bound(bytes);
+      if (b != mm.end() && b->first <= bytes + bytes / 4 + kCacheMin) {
+        void* p = b->second;
+        *capacity = b->first;
+        mm.erase(b);
+        return p;
+      }
+    }
+  }
+  void* p = nullptr;
+  const double t0 = trace_clock_ms();
+  cudaError_t e = cudaMallocAsync(&p, bytes, s);
+  trace_slow_call("cudaMallocAsync", bytes, t0);
+  if (e != cudaSuccess) {  // give this stream's cached blocks back to the pool and try once more
+    cudaGetLastError();
+    cache_trim_stream(s);
+    e = cudaMallocAsync(&p, bytes, s);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(DECO_ERR_ALLOC, "device allocation of " + std::to_string(bytes) +
+                                    " bytes failed: " + cudaGetErrorString(e));
+  }
+  *capacity = bytes;
+  return p;
+}
+
+void dev_free(void* p, size_t capacity, cudaStream_t s) {
+  if (!p) return;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    const bool live = g_live.count(s) != 0;
+    if (cache_on() && live && capacity >= kCacheMin) {
+      g_cache[s].emplace(capacity, p);
+      return;
+    }
+    if (!live) {  // the owning context (and maybe its stream) is gone
+      cudaFree(p);
+      return;
+    }
+  }
+  cudaFreeAsync(p, s);
+}
+
+void cache_attach_stream(cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  ++g_live[s];
+}
+
+void cache_trim_stream(cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  auto it = g_cache.find(s);
+  if (it == g_cache.end()) return;
+  for (auto& kv : it->second) cudaFreeAsync(kv.second, s);
+  g_cache.erase(it);
+}
+
+void cache_detach_stream(cudaStream_t s) {
+  cache_trim_stream(s);
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  auto it = g_live.find(s);
+  if (it != g_live.end() && --it->second <= 0) g_live.erase(it);
+}
+
+static bool trace_env() {
+  static const bool on = [] {
+    const char* e = std::getenv("DECO_TRACE");
+    return e && std::atoi(e) != 0;
+  }();
+  return on;
+}
+
+double trace_clock_ms() {
+  if (!trace_env()) return 0.0;
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+void trace_slow_call(const char* what, size_t bytes, double t0_ms) {
+  if (!trace_env()) return;
+  const double dt = trace_clock_ms() - t0_ms;
+  if (dt > 5.0) std::fprintf(stderr, "[deco-trace] slow %s of %.1f MB: %.1f ms\n", what, bytes / 1e6, dt);
+}
+
+void trace_mark(deco_ctx_s* ctx, const char* label) {
+  if (!ctx->trace) return;
+  cudaStreamSynchronize(ctx->stream);
+  const double t =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+  if (label) {
+    size_t reserved = 0, used = 0;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+    }
+    std::fprintf(stderr, "[deco-trace] %-28s %9.3f ms  pool %.2f/%.2f GB\n", label, t - ctx->trace_t, used / 1e9,
+                 reserved / 1e9);
+  }
+  ctx->trace_t = t;
+}
 
 namespace {
 
@@ -148,12 +274,14 @@ int deco_ctx_create(int device, void* stream, deco_ctx* out) {
     // DECO_AUTOTUNE=0 keeps the heuristic SpMV widths (profiler runs distort timings)
     if (const char* e = std::getenv("DECO_AUTOTUNE")) c->autotune = std::atoi(e) != 0;
     if (const char* e = std::getenv("DECO_BSR")) c->bsr = std::atoi(e) != 0;
+    if (const char* e = std::getenv("DECO_TRACE")) c->trace = std::atoi(e) != 0;
     // keep freed device memory in the stream-ordered pool instead of returning it
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
       unsigned long long threshold = ~0ULL;
       cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
     }
+    cache_attach_stream(c->stream);
     DECO_CUDA(cudaEventCreate(&c->ev0));
     DECO_CUDA(cudaEventCreate(&c->ev1));
     DECO_CUDA(cudaMallocHost(&c->host_scalars, 1024 * sizeof(double)));
@@ -174,6 +302,8 @@ int deco_ctx_destroy(deco_ctx ctx) {
     if (ctx->host_scalars) cudaFreeHost(ctx->host_scalars);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    cache_detach_stream(ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
   });
@@ -190,6 +320,13 @@ int deco_ctx_stream(deco_ctx ctx, void** stream) {
   return guard([&] {
     DECO_REQUIRE(ctx && stream, DECO_ERR_ARG, "NULL argument");
     *stream = ctx->stream;
+  });
+}
+
+int deco_ctx_trim(deco_ctx ctx) {
+  return guard([&] {
+    DECO_REQUIRE(ctx, DECO_ERR_ARG, "ctx is NULL");
+    cache_trim_stream(ctx->stream);
   });
 }
 

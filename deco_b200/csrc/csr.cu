@@ -74,6 +74,7 @@ __global__ void bsr_fill(int nbr, int bs, const int* __restrict__ r, const int* 
 void drop_bsr(deco_csr_s* A) {
   A->bbs = 0;
   A->nblk = 0;
+  A->bplane = 0;
   A->br = DevBuf<int>();
   A->bc = DevBuf<int>();
   A->bv = DevBuf<double>();
@@ -96,7 +97,8 @@ void make_bsr(deco_ctx_s* ctx, deco_csr_s* A, int bs, double max_fill) {
   A->br = std::move(br);
   A->nblk = (int)nblk;
   A->bc.alloc(nblk, st);
-  const long long plane = nblk * bs;
+  const long long plane = (nblk * bs + 3) / 4 * 4;
+  A->bplane = plane;
   A->bv.alloc(plane * bs, st);
   A->bv.zero(st);
   bsr_fill<<<g, 256, 0, st>>>(nbr, bs, A->r.get(), A->c.get(), A->v.get(), A->br.get(), A->bc.get(), A->bv.get(),
@@ -128,7 +130,7 @@ void make_f32_values(deco_ctx_s* ctx, deco_csr_s* A) {
   to_f32<<<grid_for(ctx, A->nz, 256), 256, 0, ctx->stream>>>(A->v.get(), A->v32.get(), A->nz);
   DECO_CHECK_LAUNCH();
   if (A->bbs) {
-    const long long nv = (long long)A->nblk * A->bbs * A->bbs;
+    const long long nv = A->bplane * A->bbs;
     if (!A->bv32 || A->bv32.size() != (size_t)nv) A->bv32.alloc(nv, ctx->stream);
     to_f32<<<grid_for(ctx, nv, 256), 256, 0, ctx->stream>>>(A->bv.get(), A->bv32.get(), nv);
     DECO_CHECK_LAUNCH();
@@ -143,8 +145,9 @@ static std::mutex g_tuned_mu;
 int tuned_bsr_subwarp(deco_ctx_s* ctx, deco_csr_s* A, bool f32) {
   int& sw = f32 ? A->bsw32 : A->bsw64;
   if (sw) return sw;
+  // about two blocks per lane: the 2 x 2 kernel moves a pair of blocks per lane step
   sw = 1;
-  while (sw < 16 && sw < A->avg_blk / 2.0) sw <<= 1;
+  while (sw < 16 && sw < A->avg_blk / (A->bbs == 2 ? 4.0 : 2.0)) sw <<= 1;
   const int nbr = A->n / A->bbs;
   if (!ctx->autotune || nbr < 4096) return sw;
   const auto key = std::make_tuple(A->n, A->m, A->nblk, -A->bbs, f32);
@@ -180,7 +183,7 @@ int tuned_bsr_subwarp(deco_ctx_s* ctx, deco_csr_s* A, bool f32) {
   float best = t_base;
   int best_sw = base;
   for (int cand : {base / 2, base * 2}) {
-    if (cand < 1 || cand > 16) continue;
+    if (cand < 1 || cand > (A->bbs == 2 ? 8 : 16)) continue;
     const float tc = time_width(cand);
     if (tc < best) { best = tc; best_sw = cand; }
   }

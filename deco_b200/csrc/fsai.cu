@@ -483,17 +483,22 @@ void csr_filter(deco_ctx_s* ctx, const deco_csr_s* A, double tol_rel, double tol
   const int n = A->n;
   DevBuf<int> cnt(n + 1, st);
   const int g = grid_for(ctx, n, 256);
+  trace_mark(ctx, "filter: count buffer");
   filter_count<<<g, 256, 0, st>>>(n, A->r.get(), A->c.get(), A->v.get(), tol_rel, tol_abs, cnt.get());
   DECO_CHECK_LAUNCH();
+  trace_mark(ctx, "filter: count");
   out->n = n;
   out->m = A->m;
   out->r.alloc(n + 1, st);
   out->nz = (int)exclusive_scan_int(ctx, cnt.get(), out->r.get(), n);
+  trace_mark(ctx, "filter: scan");
   out->c.alloc(out->nz, st);
   out->v.alloc(out->nz, st);
+  trace_mark(ctx, "filter: allocate");
   filter_copy<<<g, 256, 0, st>>>(n, A->r.get(), A->c.get(), A->v.get(), tol_rel, tol_abs, out->r.get(),
                                  out->c.get(), out->v.get());
   DECO_CHECK_LAUNCH();
+  trace_mark(ctx, "filter: copy");
   refresh_stats(ctx, out);
 }
 
@@ -542,6 +547,7 @@ void fsai_build(deco_ctx_s* ctx, const deco_csr_s* A0, double tol_rel, double to
   DECO_REQUIRE(power == 1, DECO_ERR_UNSUPPORTED, "FSAI power 2 (lower(A^2) pattern) is not available on the GPU path");
   DECO_REQUIRE(precision == 64 || precision == 32, DECO_ERR_ARG, "precision must be 64 or 32");
   const int n = A0->n;
+  trace_mark(ctx, nullptr);
   F->n = n;
   F->precision = precision;
   // 1. filtered copy (FSAI.hpp:22-28)
@@ -552,6 +558,7 @@ void fsai_build(deco_ctx_s* ctx, const deco_csr_s* A0, double tol_rel, double to
     A = &Af;
   }
   const int g = grid_for(ctx, n, 256);
+  trace_mark(ctx, "fsai filter");
   // 2. symbolic: lower(A)
   DevBuf<int> cnt(n + 1, st);
   lower_count<<<g, 256, 0, st>>>(n, A->r.get(), A->c.get(), cnt.get());
@@ -568,6 +575,7 @@ void fsai_build(deco_ctx_s* ctx, const deco_csr_s* A0, double tol_rel, double to
   F->nz = FL.nz;
   DevBuf<double> fu(FL.nz, st);  // FU values in FL's (lower) layout before the transpose
   fu.zero(st);
+  trace_mark(ctx, "fsai symbolic");
   // 3. group rows by order and solve the local systems in one launch
   DevBuf<int> hist(16, st);
   hist.zero(st);
@@ -596,17 +604,21 @@ void fsai_build(deco_ctx_s* ctx, const deco_csr_s* A0, double tol_rel, double to
                                                                 FL.v.get(), fu.get());
     DECO_CHECK_LAUNCH();
   }
+  trace_mark(ctx, "fsai local systems");
   // 4. D = diag(FL A FU^T); FL *= D, FU *= |D|  (diagonal.cpp:6-73)
   fsai_scale<<<g, 256, 0, st>>>(n, A->r.get(), A->c.get(), A->v.get(), FL.r.get(), FL.c.get(), FL.v.get(), fu.get());
   DECO_CHECK_LAUNCH();
+  trace_mark(ctx, "fsai scaling");
   // 5. FU^T (trans_mat_full)
   deco_csr_s& U = F->FUt;
   csr_transpose(ctx, n, n, FL.nz, FL.r.get(), FL.c.get(), fu.get(), &U);
   refresh_stats(ctx, &FL);
+  trace_mark(ctx, "fsai transpose");
   if (bs > 1) {
     make_bsr(ctx, &FL, bs);
     make_bsr(ctx, &U, bs);
   }
+  trace_mark(ctx, "fsai block copies");
   F->tmp.alloc(n, st);
   if (precision == 32) {
     make_f32_values(ctx, &FL);
@@ -614,6 +626,7 @@ void fsai_build(deco_ctx_s* ctx, const deco_csr_s* A0, double tol_rel, double to
     F->tmp32.alloc(n, st);
   }
   DECO_CUDA(cudaStreamSynchronize(st));
+  trace_mark(ctx, "fsai f32 copies");
 }
 
 }  // namespace deco

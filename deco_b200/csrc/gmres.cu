@@ -392,6 +392,7 @@ struct Solver {
   }
 
   Solver(deco_ctx_s* c, deco_csr_s* a, deco_cpr_s* p, const deco_sol_params& pr) : ctx(c), A(a), P(p), prm(pr) {
+    trace_mark(ctx, "gmres: enter");
     n = A->n;
     ld = (n + 31) / 32 * 32;
     m = prm.restart;
@@ -413,6 +414,7 @@ struct Solver {
       pev.resize(4 * (size_t)(m + 1));
       for (auto& e : pev) DECO_CUDA(cudaEventCreate(&e));
     }
+    trace_mark(ctx, "gmres: allocate");
   }
 
   // adds the phase times of steps [0, steps) of the cycle that just finished
@@ -582,6 +584,7 @@ struct Solver {
     DECO_CUDA(cudaEventSynchronize(ctx->ev1));
     float ms = 0.f;
     DECO_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    trace_mark(ctx, "gmres: solve");
     res->iter = iter;
     res->flag = flag;
     res->res_abs = rnorm;

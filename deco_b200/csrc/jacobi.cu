@@ -28,18 +28,18 @@ __global__ void jacobi_setup(int sn, const int* __restrict__ r, const int* __res
       const int i = s * BS + p, ia = r[i], ib = r[i + 1];
       if (ib <= ia) continue;
       const int j = find_diag(c, ia, ib, i);
-      if (BS == 1) {
+      if constexpr (BS == 1) {
         B[0][0] = v[j];
-        continue;
-      }
-      for (int k = 0; k < BS; ++k) {
-        const int q = j + k - p;
-        if (q < ia || q >= ib) continue;
-        if (c[q] / BS == s) B[p][c[q] % BS] = v[q];
+      } else {
+        for (int k = 0; k < BS; ++k) {
+          const int q = j + k - p;
+          if (q < ia || q >= ib) continue;
+          if (c[q] / BS == s) B[p][c[q] % BS] = v[q];
+        }
       }
     }
     double* out = J + (long long)s * BS * BS;
-    if (BS == 1) {  // no check, as Jacobi::classic: a zero diagonal gives inf
+    if constexpr (BS == 1) {  // no check, as Jacobi::classic: a zero diagonal gives inf
       out[0] = 1.0 / B[0][0];
       continue;
     }

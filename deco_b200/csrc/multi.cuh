@@ -1,0 +1,194 @@
+// multi.cuh — products with K right-hand sides at once, for the batched solve.
+//
+// Multi-vectors are row-interleaved: X[row * K + k], so the K values a matrix
+// entry multiplies sit in one 32-byte (float) or 64-byte (double) segment and
+// every entry of the matrix is read once for all K columns.  The kernel is the
+// cell-block product of spmv.cuh widened to K columns: a sub-warp of SW lanes
+// owns a block row (BS matrix rows), lanes take whole blocks, and the BS x K
+// sums of the block row stay in registers until the sub-warp reduction; then
+// the lanes share the NR x K epilogue writes.  A scalar CSR matrix is the BS = 1
+// case (one column index per entry, one value plane).
+#pragma once
+#include "spmv.cuh"
+
+namespace deco {
+
+// ------------------------------------------------------------ epilogues
+// epi(row, k, value): value = (A X)[row][k] (row = cell for a restricted product)
+template <int K, typename YT> struct MStore {
+  YT* y;
+  __device__ void operator()(int row, int k, double v) const { y[(long long)row * K + k] = (YT)v; }
+};
+template <int K, typename YT> struct MAdd {
+  YT* y;
+  __device__ void operator()(int row, int k, double v) const {
+    const long long o = (long long)row * K + k;
+    y[o] = (YT)((double)y[o] + v);
+  }
+};
+template <int K, typename ZT, typename YT> struct MResid {  // y = z - A x
+  const ZT* z; YT* y;
+  __device__ void operator()(int row, int k, double v) const {
+    const long long o = (long long)row * K + k;
+    y[o] = (YT)((double)z[o] - v);
+  }
+};
+template <int K, typename ZT, typename YT> struct MRestrict {  // y[s] = r[s*bs+p] - (A x)[s*bs]
+  const ZT* r; YT* y; int bs, p;
+  __device__ void operator()(int s, int k, double v) const {
+    y[(long long)s * K + k] = (YT)((double)r[((long long)s * bs + p) * K + k] - v);
+  }
+};
+template <int K, typename YT> struct MProlong {  // x[s*bs+p] += (F t)[s]
+  YT* x; int bs, p;
+  __device__ void operator()(int s, int k, double v) const {
+    const long long o = ((long long)s * bs + p) * K + k;
+    x[o] = (YT)((double)x[o] + v);
+  }
+};
+// y = scale[q] * (A x) with q = system(row) * K + k: the per-instance scale of the
+// lazily normalised basis column (scale[q * stride]); cell_sys maps a cell
+// (bs rows) to its system
+template <int K, typename YT> struct MStoreScaled {
+  YT* y; const double* scale; long long stride; const int* cell_sys; int bs;
+  __device__ void operator()(int row, int k, double v) const {
+    const int sys = __ldg(cell_sys + row / bs);
+    y[(long long)row * K + k] = (YT)(__ldg(scale + (long long)(sys * K + k) * stride) * v);
+  }
+};
+
+// K consecutive values from x + o (o a multiple of K) as doubles, with 16-byte loads
+template <int K, typename XT>
+__device__ __forceinline__ void load_k(const XT* __restrict__ x, long long o, double* out) {
+  if constexpr (sizeof(XT) == 4 && K % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < K / 4; ++q) {
+      const float4 t = __ldg(reinterpret_cast<const float4*>(x + o) + q);
+      out[4 * q] = t.x; out[4 * q + 1] = t.y; out[4 * q + 2] = t.z; out[4 * q + 3] = t.w;
+    }
+  } else if constexpr (sizeof(XT) == 8 && K % 2 == 0) {
+#pragma unroll
+    for (int q = 0; q < K / 2; ++q) {
+      const double2 t = __ldg(reinterpret_cast<const double2*>(x + o) + q);
+      out[2 * q] = t.x; out[2 * q + 1] = t.y;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < K; ++q) out[q] = (double)__ldg(x + o + q);
+  }
+}
+
+// ------------------------------------------------------------ the kernel
+template <int SW, int BS, int K, bool ROW0, typename VT, typename XT, class Epi>
+__global__ void __launch_bounds__(256) bsr_mm_kernel(int nbr, const int* __restrict__ br, const int* __restrict__ bc,
+                                                     const VT* __restrict__ bv, long long plane,
+                                                     const XT* __restrict__ x, Epi epi) {
+  constexpr int NR = ROW0 ? 1 : BS;
+  const int lane = threadIdx.x & (SW - 1);
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = int(gid / SW);
+  const bool valid = s < nbr;
+  double acc[NR][K];
+#pragma unroll
+  for (int q = 0; q < NR; ++q)
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[q][k] = 0.0;
+  if (valid) {
+    const int a = __ldg(br + s), e = __ldg(br + s + 1);
+    for (int blk = a + lane; blk < e; blk += SW) {
+      const long long col0 = (long long)__ldcs(bc + blk) * BS;
+#pragma unroll
+      for (int t = 0; t < BS; ++t) {
+        double xv[K];
+        load_k<K, XT>(x, (col0 + t) * K, xv);
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+          const double w = (double)__ldcs(bv + q * plane + (long long)blk * BS + t);
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[q][k] += w * xv[k];
+        }
+      }
+    }
+  }
+  if (SW > 1) {
+#pragma unroll
+    for (int q = 0; q < NR; ++q)
+#pragma unroll
+      for (int k = 0; k < K; ++k) acc[q][k] = subwarp_sum<SW>(acc[q][k]);
+  }
+  if (!valid) return;
+#pragma unroll
+  for (int q = 0; q < NR; ++q)
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if ((q * K + k) % SW == lane) epi(ROW0 ? s : s * BS + q, k, acc[q][k]);
+}
+
+// A matrix for the K-column product: its cell-block copy when it has one
+// (BS = bbs), else the CSR arrays as BS = 1 blocks.
+struct MMView {
+  int bs, nbr;
+  const int* br;
+  const int* bc;
+  long long plane;
+  const double* v64;
+  const float* v32;
+  int sw;
+};
+
+inline MMView mm_view(const deco_csr_s* A) {
+  MMView m{};
+  if (A->bbs > 1) {
+    m.bs = A->bbs; m.nbr = A->n / A->bbs; m.br = A->br.get(); m.bc = A->bc.get();
+    m.plane = A->bplane; m.v64 = A->bv.get(); m.v32 = A->bv32.get();
+    m.sw = 1;
+    while (m.sw < 16 && m.sw < A->avg_blk / 2.0) m.sw <<= 1;
+  } else {
+    m.bs = 1; m.nbr = A->n; m.br = A->r.get(); m.bc = A->c.get(); m.plane = A->nz;
+    m.v64 = A->v.get(); m.v32 = A->v32.get();
+    m.sw = 1;
+    while (m.sw < 16 && m.sw < A->avg_row / 2.0) m.sw <<= 1;
+  }
+  return m;
+}
+
+template <int SW, int BS, int K, bool ROW0, typename VT, typename XT, class Epi>
+void launch_mm_sw(cudaStream_t st, const MMView& M, const VT* v, const XT* x, Epi epi) {
+  const unsigned grid = (unsigned)cdiv((long long)M.nbr * SW, 256);
+  bsr_mm_kernel<SW, BS, K, ROW0, VT, XT, Epi><<<grid, 256, 0, st>>>(M.nbr, M.br, M.bc, v, M.plane, x, epi);
+  DECO_CHECK_LAUNCH();
+}
+
+template <int BS, int K, bool ROW0, typename VT, typename XT, class Epi>
+void launch_mm_bs(cudaStream_t st, const MMView& M, const VT* v, const XT* x, Epi epi) {
+  switch (M.sw) {
+    case 1: launch_mm_sw<1, BS, K, ROW0>(st, M, v, x, epi); break;
+    case 2: launch_mm_sw<2, BS, K, ROW0>(st, M, v, x, epi); break;
+    case 4: launch_mm_sw<4, BS, K, ROW0>(st, M, v, x, epi); break;
+    case 8: launch_mm_sw<8, BS, K, ROW0>(st, M, v, x, epi); break;
+    default: launch_mm_sw<16, BS, K, ROW0>(st, M, v, x, epi); break;
+  }
+}
+
+// Y = op(A X) with K columns; row0: the restricted product over row 0 of every
+// cell of size `bs` (A must then have a cell-block copy of that size, or bs = 1).
+template <int K, typename VT, typename XT, class Epi>
+void spmm(deco_ctx_s* ctx, const deco_csr_s* A, const XT* x, Epi epi, bool row0 = false, int sw = 0) {
+  MMView M = mm_view(A);
+  if (sw) M.sw = sw;
+  const VT* v;
+  if constexpr (sizeof(VT) == 4) v = M.v32; else v = M.v64;
+  DECO_REQUIRE(v != nullptr, DECO_ERR_INTERNAL, "matrix values of the requested precision are missing");
+  DECO_REQUIRE(!row0 || M.bs > 1, DECO_ERR_INTERNAL, "restricted K-column product needs a cell-block copy");
+  cudaStream_t st = ctx->stream;
+  if (M.bs == 1) launch_mm_bs<1, K, false, VT, XT, Epi>(st, M, v, x, epi);
+  else if (M.bs == 2) {
+    if (row0) launch_mm_bs<2, K, true, VT, XT, Epi>(st, M, v, x, epi);
+    else launch_mm_bs<2, K, false, VT, XT, Epi>(st, M, v, x, epi);
+  } else {
+    if (row0) launch_mm_bs<3, K, true, VT, XT, Epi>(st, M, v, x, epi);
+    else launch_mm_bs<3, K, false, VT, XT, Epi>(st, M, v, x, epi);
+  }
+}
+
+}  // namespace deco

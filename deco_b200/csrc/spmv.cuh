@@ -33,8 +33,9 @@ struct deco_csr_s {
   // in-block row q of every block) so a product over row 0 of each cell reads
   // one plane only.  bbs == 0: no block copy.
   int bbs = 0, nblk = 0;
+  long long bplane = 0;       // plane stride in values: nblk * bbs rounded up to 4 (16-byte aligned planes)
   deco::DevBuf<int> br, bc;   // block-row pointers (n / bbs + 1), block columns
-  deco::DevBuf<double> bv;    // bbs planes of nblk * bbs values
+  deco::DevBuf<double> bv;    // bbs planes of bplane values
   deco::DevBuf<float> bv32;
   int bsw64 = 0, bsw32 = 0;
   double avg_blk = 0;
@@ -200,9 +201,84 @@ __global__ void __launch_bounds__(256) bsr_kernel(int nbr, const int* __restrict
   }
 }
 
+// 2 x 2 cells: each lane takes a PAIR of consecutive blocks per step, from the
+// pair-aligned start of the block row, with one 8-byte load of their two columns
+// and one 16-byte (float) or two 16-byte (double) loads of their values per
+// plane; blocks outside the row are masked (their loads stay inside the padded
+// arrays: the planes are 16-byte aligned and the index array has slack).
+template <typename T> struct Quad;
+template <> struct Quad<float> {
+  __device__ static void load(const float* p, double* o) {
+    const float4 t = __ldcs(reinterpret_cast<const float4*>(p));
+    o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
+  }
+};
+template <> struct Quad<double> {
+  __device__ static void load(const double* p, double* o) {
+    const double2 t = __ldcs(reinterpret_cast<const double2*>(p));
+    const double2 u = __ldcs(reinterpret_cast<const double2*>(p) + 1);
+    o[0] = t.x; o[1] = t.y; o[2] = u.x; o[3] = u.y;
+  }
+};
+
+template <int SW, bool ROW0, typename VT, typename XT, class Epi>
+__global__ void __launch_bounds__(256) bsr2_pair_kernel(int nbr, const int* __restrict__ br, const int* __restrict__ bc,
+                                                        const VT* __restrict__ bv, long long plane,
+                                                        const XT* __restrict__ x, Epi epi) {
+  const int lane = threadIdx.x & (SW - 1);
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = int(gid / SW);
+  const bool valid = s < nbr;
+  double s0 = 0.0, s1 = 0.0;
+  if (valid) {
+    const int a = __ldg(br + s), e = __ldg(br + s + 1);
+    for (int k = (a & ~1) + 2 * lane; k < e; k += 2 * SW) {
+      const int2 c2 = __ldcs(reinterpret_cast<const int2*>(bc + k));
+      double w0[4], w1[4];
+      Quad<VT>::load(bv + 2LL * k, w0);
+      if (!ROW0) Quad<VT>::load(bv + plane + 2LL * k, w1);
+      if (k >= a) {
+        const typename Pair<XT>::V p = __ldg(reinterpret_cast<const typename Pair<XT>::V*>(x + 2LL * c2.x));
+        s0 += w0[0] * (double)p.x;
+        s0 += w0[1] * (double)p.y;
+        if (!ROW0) { s1 += w1[0] * (double)p.x; s1 += w1[1] * (double)p.y; }
+      }
+      if (k + 1 < e) {
+        const typename Pair<XT>::V p = __ldg(reinterpret_cast<const typename Pair<XT>::V*>(x + 2LL * c2.y));
+        s0 += w0[2] * (double)p.x;
+        s0 += w0[3] * (double)p.y;
+        if (!ROW0) { s1 += w1[2] * (double)p.x; s1 += w1[3] * (double)p.y; }
+      }
+    }
+  }
+  if (SW > 1) {
+    s0 = subwarp_sum<SW>(s0);
+    if (!ROW0) s1 = subwarp_sum<SW>(s1);
+  }
+  if (valid && lane == 0) {
+    if (ROW0) {
+      epi(s, s0);
+    } else {
+      epi(2 * s, s0);
+      epi(2 * s + 1, s1);
+    }
+  }
+}
+
 template <int BS, bool ROW0, typename VT, typename XT, class Epi>
 void launch_bsr_bs(cudaStream_t st, int sw, int nbr, const int* br, const int* bc, const VT* bv, long long plane,
                    const XT* x, Epi epi) {
+  if constexpr (BS == 2) {
+    const unsigned grid = (unsigned)cdiv((long long)nbr * sw, 256);
+    switch (sw) {
+      case 1: bsr2_pair_kernel<1, ROW0, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, br, bc, bv, plane, x, epi); break;
+      case 2: bsr2_pair_kernel<2, ROW0, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, br, bc, bv, plane, x, epi); break;
+      case 4: bsr2_pair_kernel<4, ROW0, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, br, bc, bv, plane, x, epi); break;
+      default: bsr2_pair_kernel<8, ROW0, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, br, bc, bv, plane, x, epi); break;
+    }
+    DECO_CHECK_LAUNCH();
+    return;
+  }
   const int block = 256;
   const unsigned grid = (unsigned)cdiv((long long)nbr * sw, block);
   switch (sw) {
@@ -223,7 +299,7 @@ void launch_bsr(cudaStream_t st, const deco_csr_s* A, int sw, bool row0, const X
   if (nbr <= 0) return;
   const VT* bv;
   if constexpr (sizeof(VT) == 4) bv = A->bv32.get(); else bv = A->bv.get();
-  const long long plane = (long long)A->nblk * A->bbs;
+  const long long plane = A->bplane;
   if (A->bbs == 2) {
     if (row0) launch_bsr_bs<2, true, VT, XT, Epi>(st, sw, nbr, A->br.get(), A->bc.get(), bv, plane, x, epi);
     else launch_bsr_bs<2, false, VT, XT, Epi>(st, sw, nbr, A->br.get(), A->bc.get(), bv, plane, x, epi);

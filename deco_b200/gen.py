@@ -139,3 +139,34 @@ def grid(nx: int, ny: int, nz: int, bs: int = 2, seed: int = 1234, **kw) -> Syst
     for k, val in kw.items():
         setattr(p, k, val)
     return generate(p)
+
+
+def batch(nsys: int = 64, seed: int = 1234, cells_lo: int = 10_000, cells_hi: int = 500_000, bs: int = 2,
+          nrhs: int = 8):
+    """Independent two-phase systems (the config-1 value distributions) with cell
+    counts drawn log-uniform in [cells_lo, cells_hi], concatenated into one
+    block-diagonal CSR, plus `nrhs` uniform [0,1) right-hand sides per system
+    (row-interleaved).  Returns (r, c, v, row_off, B, shapes)."""
+    u = uniform(seed, 911, 2 * nsys)
+    rs, cs, vs, offs, shapes = [], [], [], [0], []
+    nz_off = 0
+    for q in range(nsys):
+        cells = float(np.exp(np.log(cells_lo) + u[q] * (np.log(cells_hi) - np.log(cells_lo))))
+        nzc = max(2, int(round((cells / 4.0) ** (1.0 / 3.0))))  # nx = ny = 2 nz
+        nxy = max(2, int(round(np.sqrt(cells / nzc))))
+        p = preset(1, seed + 7919 * (q + 1))
+        p.nx, p.ny, p.nz, p.bs = nxy, nxy, nzc, bs
+        s = generate(p)
+        shapes.append((nxy, nxy, nzc))
+        rs.append(s.r[:-1] + nz_off)
+        cs.append(s.c + offs[-1])
+        vs.append(s.v)
+        nz_off += s.nnz
+        offs.append(offs[-1] + s.n)
+    r = np.concatenate(rs + [np.array([nz_off], np.int64)]).astype(np.int32)
+    c = np.concatenate(cs).astype(np.int32)
+    v = np.concatenate(vs)
+    row_off = np.array(offs, np.int32)
+    n = int(row_off[-1])
+    B = uniform(seed, 913, n * nrhs)
+    return r, c, v, row_off, B, shapes

@@ -64,6 +64,11 @@ int deco_ctx_sync(deco_ctx ctx);
 int deco_ctx_stream(deco_ctx ctx, void** stream);
 /* autotune != 0: SpMV sub-warp width is chosen per matrix by timing (default 1). */
 int deco_ctx_set_autotune(deco_ctx ctx, int autotune);
+/* Returns the device blocks the context keeps for reuse to the device's memory
+ * pool.  Blocks of 1 MiB and more that the library frees stay cached per
+ * stream and serve later requests on that stream (no counterpart in the
+ * reference, which allocates host memory with malloc). */
+int deco_ctx_trim(deco_ctx ctx);
 
 /* --------------------------------------------------------------- matrices
  * Replaces CSR<int,int,double> construction and its raw arrays
@@ -255,6 +260,47 @@ int deco_adjoint_solve(deco_ctx ctx, deco_adjoint J, const double* d_g, double* 
 /* The transposed matrix (decoupled in place by the adjoint's CPR) and its
  * preconditioner, owned by J. */
 int deco_adjoint_parts(deco_adjoint J, deco_csr* At, deco_cpr* P);
+
+/* ------------------------------------------------------------ batched solve
+ * Many independent systems, each with nrhs right-hand sides, solved together
+ * (no counterpart in the reference).  The systems are one block-diagonal
+ * matrix A: system q owns rows [h_row_off[q], h_row_off[q+1]) (cell-aligned)
+ * and references only its own columns.  deco_batch_create builds ONE CPR on A
+ * (decoupling A in place, as deco_cpr_create), which is every system's CPR at
+ * once.  Right-hand sides and solutions are row-interleaved multi-vectors:
+ * B[row * nrhs + k].  Every (system, column) pair is an rgmres(m) instance with
+ * its own Hessenberg matrix, rotations, convergence checks (inner and outer,
+ * rgmres.tpp:58-66,118-123) and iteration limit; all instances advance in
+ * lockstep through products that read the matrix once for all columns, and a
+ * restart cycle runs as one CUDA graph. */
+typedef struct deco_batch_s* deco_batch;
+
+typedef struct deco_batch_result {
+  int max_iter;          /* largest inner iteration count over the instances  */
+  int converged;         /* instances with flag 0                             */
+  int cycles;            /* restart cycles run                                */
+  int graph;             /* 1: the cycles ran as a captured CUDA graph        */
+  double t_solve_ms;     /* device time of the solve                          */
+} deco_batch_result;
+
+/* nrhs: 1, 2, 4 or 8.  prm: CPR seq 0 or 3 with FSAI stages; the systems must
+ * consist of dense bs x bs cell blocks (their products use cell-block copies). */
+int deco_batch_create(deco_ctx ctx, deco_csr A, int nsys, const int* h_row_off, int nrhs,
+                      const deco_cpr_params* prm, deco_batch* out);
+int deco_batch_destroy(deco_batch B);
+/* h_widths (optional, nsys ints): the product width chosen for each system. */
+int deco_batch_info(deco_batch B, int* nsys, int* nrhs, int* nchunk, int* h_widths);
+int deco_batch_cpr(deco_batch B, deco_cpr* P);
+/* X = M^{-1} R for every system and column with the batch's CPR (float64 in and
+ * out; precision 32 runs the float32 preconditioner, as at a GMRES restart). */
+int deco_batch_apply(deco_ctx ctx, deco_batch B, const double* d_R, double* d_X);
+/* Solves every instance from x = 0.  d_B: the ORIGINAL right-hand sides (not
+ * decoupled; they are decoupled into scratch by the recorded row operations).
+ * prm.type must be rgmres and prm.precision the CPR's.  Optional host outputs,
+ * nsys * nrhs each in (system, column) order: iterations, final true relative
+ * residual of the decoupled system, flag. */
+int deco_batch_solve(deco_ctx ctx, deco_batch B, const double* d_B, double* d_X, const deco_sol_params* prm,
+                     int* h_iters, double* h_res_rel, int* h_flags, deco_batch_result* res);
 
 #ifdef __cplusplus
 }

@@ -212,9 +212,12 @@ def test_cpr_errors(d):
     with pytest.raises(d.DecoError) as e:
         d.CPR(cpr_json(2), A, cuda(s.b))
     assert e.value.code == -4
-    # seq 2 needs block Jacobi: reported as unsupported
+    # an unknown sequence is an argument error; hypre AMG stays on the CPU build
     with pytest.raises(d.DecoError) as e:
-        d.CPR(cpr_json(2, seq=2), d.CSR.from_system(s), cuda(s.b))
+        d.CPR(cpr_json(2, seq=4), d.CSR.from_system(s), cuda(s.b))
+    assert e.value.code == -1
+    with pytest.raises(d.DecoError) as e:
+        d.CPR(cpr_json(2, loc="hypre_AMG"), d.CSR.from_system(s), cuda(s.b))
     assert e.value.code == -6
 
 
