@@ -164,14 +164,26 @@ def run_reference(args, rank, world):
 
 def bench_batch(args):
     """64 independent two-phase systems (cells log-uniform in 10k-500k), 8
-    right-hand sides each, one lockstep CPR-GMRES solve per precision."""
+    right-hand sides each, one lockstep CPR-GMRES solve per precision.  Under
+    torchrun the systems are dealt round-robin to the ranks (independent systems:
+    no collective on the data path); the time is the max over ranks."""
+    import datetime
     import torch
     import deco_b200 as d
-    from deco_b200 import gen
-    ctx = d.Context(0)
+    from deco_b200 import gen, replicas
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    ctx = d.Context(int(os.environ.get("LOCAL_RANK", 0)))
     st = ctx.torch_stream
     torch.cuda.set_stream(st)
     r, c, v, ro, B, shapes = gen.batch(64, SEED, 10_000, 500_000, 2, 8)
+    n_all, nnz_all = int(ro[-1]), len(c)
+    if world > 1:
+        r, c, v, ro, B = gen.batch_subset(r, c, v, ro, B, 8, list(range(rank, 64, world)))
     n, nnz = int(ro[-1]), len(c)
     dev = lambda a: torch.from_numpy(a).cuda()
     r_d, c_d, v_d, B_d = dev(r), dev(c), dev(v), dev(B)
@@ -189,22 +201,89 @@ def bench_batch(args):
             if k >= args.warmup:
                 rows.append((e0.elapsed_time(e1), Bt.result, Bt.iters.copy(), Bt.res_rel.copy(), Bt.widths.copy()))
             del Bt, A, X
-        ms = statistics.mean(t[0] for t in rows)
+        ms = replicas.max_over_ranks(statistics.mean(t[0] for t in rows), device="cuda")
         res, it, rr, w = rows[-1][1], rows[-1][2], rows[-1][3], rows[-1][4]
+        inst = int(replicas.sum_over_ranks(it.size, device="cuda"))
         out["mixed" if bits == 32 else "fp64"] = {
             "time_s": ms / 1e3, "solve_ms": res["t_solve_ms"], "cycles": res["cycles"], "graph": res["graph"],
-            "converged": res["converged"], "instances": int(it.size), "iterations_max": int(it.max()),
-            "iterations_median": float(statistics.median(it.ravel().tolist())),
-            "max_true_rel_residual": float(rr.max()), "widths": sorted(set(int(x) for x in w)),
-            "instances_per_s": it.size / (ms / 1e3)}
+            "converged": int(replicas.sum_over_ranks(res["converged"], device="cuda")), "instances": inst,
+            "iterations_max": int(replicas.max_over_ranks(int(it.max()), device="cuda")),
+            "iterations_median_rank0": float(statistics.median(it.ravel().tolist())),
+            "max_true_rel_residual": replicas.max_over_ranks(float(rr.max()), device="cuda"),
+            "widths": sorted(set(int(x) for x in w)), "instances_per_s": inst / (ms / 1e3)}
     line = {"metric": "batched CPR-GMRES time-to-1e-8 (64 systems x 8 right-hand sides)",
-            "value": out["mixed"]["time_s"], "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "higher_is_better": False, "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": f"config 4: 64 two-phase systems, cells log-uniform 10k-500k ({n // 2} cells, "
-                                   f"{n} rows, {nnz} nnz), 8 uniform right-hand sides each; CPR seq 3 + GMRES(50)",
-                       "seed": SEED}, **out,
+            "value": out["mixed"]["time_s"], "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": False, "scaling": "strong", "dtype": "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": f"config 4: 64 two-phase systems, cells log-uniform 10k-500k ({n_all // 2} cells, "
+                                   f"{n_all} rows, {nnz_all} nnz), 8 uniform right-hand sides each; CPR seq 3 + "
+                                   f"GMRES(50)", "seed": SEED,
+                       "parallelism": f"systems dealt round-robin to {world} GPU(s), no collective"}, **out,
             "speedup_mixed_vs_fp64": out["fp64"]["time_s"] / out["mixed"]["time_s"]}
-    print(json.dumps(line))
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def bench_spmv(args):
+    """The SpMV of the 8M-row system alone (a few GB on the device): CSR and cell-block
+    storage, float64 and float32 values, all rows and the restricted row-0 product;
+    sized for profiler captures (`ncu -k regex:bsr2_pair`)."""
+    import torch
+    import deco_b200 as d
+    ctx = d.Context(0)
+    st = ctx.torch_stream
+    torch.cuda.set_stream(st)
+    s = make_system()
+    n, nnz = s.n, s.nnz
+    A = d.CSR.from_system(s, ctx)
+    del s
+    x64 = torch.randn(n, dtype=torch.float64, device="cuda")
+    x32 = x64.float()
+    y64 = torch.empty(n, dtype=torch.float64, device="cuda")
+    y32 = torch.empty(n, dtype=torch.float32, device="cuda")
+    yr = torch.empty(n // 2, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    reps = max(1, args.steps)
+
+    def ms(fn):
+        for _ in range(max(1, args.warmup)):
+            fn()
+        tot = 0.0
+        for _ in range(reps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            fn()
+            e1.record(st)
+            e1.synchronize()
+            tot += e0.elapsed_time(e1)
+        return tot / reps
+
+    peak, _ = peaks()
+    out = {}
+    A.apply_f32(x32, y32)
+    for fmt in ("csr", "blocks"):
+        if fmt == "blocks":
+            A.set_blocks(2)
+        bsz, nblk = A.blocks
+        if bsz:
+            mat = lambda vb: nblk * 4 + nblk * 4 * vb + 4 * (n // 2 + 1)
+            row0 = nblk * 4 + nblk * 2 * 8 + 4 * (n // 2 + 1)
+        else:
+            mat = lambda vb: nnz * (4 + vb) + 4 * (n + 1)
+            row0 = nnz // 2 * 12 + 4 * (n // 2 + 1)
+        for name, fn, byt in (("f64", lambda: A.apply(x64, y64), mat(8) + 16 * n),
+                              ("f32", lambda: A.apply_f32(x32, y32), mat(4) + 8 * n),
+                              ("f64_row0", lambda: A.apply(x64, yr, bs=2), row0 + 8 * n + 4 * n)):
+            t = ms(fn)
+            out[f"{fmt}_{name}"] = {"ms": t, "gbs": byt / t / 1e6, "frac_of_peak": byt / t / 1e6 / peak, "bytes": byt}
+    print(json.dumps({"metric": "SpMV HBM GB/s on the 8M-row system", "unit": "GB/s", "n_gpus": 1, "steps": reps,
+                      "warmup": args.warmup, "data": "synthetic", "peak_gbs": peak,
+                      "config": {"workload": WORKLOAD.split(";")[0], "seed": SEED}, "kernels": out}))
 
 
 def bench_adjoint(args):
@@ -276,13 +355,16 @@ def main():
     ap.add_argument("--kernels-only", action="store_true",
                     help="only the per-kernel timings (for profiler captures on a smaller --config)")
     ap.add_argument("--config", type=int, default=3, help="system preset (3 = the benchmark workload)")
-    ap.add_argument("--workload", default="solve", choices=["solve", "batch", "adjoint"],
-                    help="solve: the headline single-system solve; batch: config 4; adjoint: config 5")
+    ap.add_argument("--workload", default="solve", choices=["solve", "batch", "adjoint", "spmv"],
+                    help="solve: the headline single-system solve; batch: config 4; adjoint: config 5; "
+                         "spmv: the SpMV kernels alone")
     args = ap.parse_args()
     if args.workload == "batch":
         return bench_batch(args)
     if args.workload == "adjoint":
         return bench_adjoint(args)
+    if args.workload == "spmv":
+        return bench_spmv(args)
     global CONFIG
     CONFIG = args.config
     rank = int(os.environ.get("RANK", 0))

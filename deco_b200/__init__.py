@@ -540,7 +540,7 @@ class Batch:
         self.res_rel = rr.reshape(self.nsys, self.nrhs)
         self.flags = fl.reshape(self.nsys, self.nrhs)
         self.result = {"max_iter": res.max_iter, "converged": res.converged, "cycles": res.cycles,
-                       "graph": bool(res.graph), "t_solve_ms": res.t_solve_ms}
+                       "graph": int(res.graph), "t_solve_ms": res.t_solve_ms}
         return X
 
     def __del__(self):

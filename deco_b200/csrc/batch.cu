@@ -19,9 +19,9 @@
 // and outer convergence checks and its iteration limit — and stops contributing
 // once converged.  A whole restart cycle (m Arnoldi steps, the back
 // substitution, the solution update and the true residual) is captured once in a
-// CUDA graph and replayed; the host reads one counter of unfinished instances per
-// cycle.  Systems whose instances have all finished are skipped by the dot,
-// update and start kernels.
+// CUDA graph that runs inside a device-side while loop (a conditional graph
+// node), so the whole solve is one graph launch.  Systems whose instances have
+// all finished are skipped by the products, dots and updates of the inner steps.
 #include <algorithm>
 #include <cmath>
 #include <type_traits>
@@ -436,6 +436,15 @@ __global__ void b_outer(int Q, const int* sch, Inst in, const double* __restrict
   if (threadIdx.x == 0) in.remaining[0] = cnt;
 }
 
+// the last kernel of a cycle inside the device-side loop: count the cycle and
+// keep looping while instances are unfinished and the cycle bound is not reached
+__global__ void b_continue(cudaGraphConditionalHandle h, const int* __restrict__ remaining, int* __restrict__ cycles,
+                           int max_cycles) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int c = ++cycles[0];
+  cudaGraphSetConditional(h, (remaining[0] > 0 && c < max_cycles) ? 1u : 0u);
+}
+
 // right-hand-side replay of the decoupling on a K-column multi-vector (cpr.cu)
 template <int K>
 __global__ void b_decouple_rhs(int sn, int bs, int weights, int use_drs, int cpd, const double* __restrict__ w0,
@@ -501,7 +510,7 @@ struct BatchSolver {
   long long n, ld, nk;
   DevBuf<T> V, w, z;
   DevBuf<double> r, xtmp, z64, bdec, stbuf, red;
-  DevBuf<int> ints, brk;
+  DevBuf<int> ints, brk, cyc;
   DevBuf<double> dres;
   BState st{};
   Inst in{};
@@ -535,6 +544,7 @@ struct BatchSolver {
     dres.alloc((size_t)2 * Q, s);
     brk.alloc(1, s);
     brk.zero(s);
+    cyc.alloc(1, s);
     in.active = ints.get();
     in.done = in.active + Q;
     in.iters = in.done + Q;
@@ -552,26 +562,30 @@ struct BatchSolver {
 
   // x = M^{-1} r on K columns (apply_seq3 / apply_seq0 of CPR.hpp:235-274, 300-325);
   // VT: value precision of the preconditioner; R/X: vector types
+  // gate: leave out the cells of systems with no running instance (inner steps
+  // only; the restart update must cover every system with a coefficient)
   template <typename VT, typename R, typename X, typename S>
-  void precond(const R* rin, X* x, S* tg_, S* tl_, S* rt_, S* rts_) {
+  void precond(const R* rin, X* x, S* tg_, S* tl_, S* rt_, S* rts_, MMGate gate = MMGate{}) {
     deco_cpr_s* P = B->P;
     const int bs = P->bs, p = P->p;
     deco_csr_s* A = P->A;
-    spmm<K, VT, R>(ctx, &P->glo.FL, rin, MStore<K, S>{tg_});
-    spmm<K, VT, S>(ctx, &P->glo.FUt, tg_, MStore<K, X>{x});
-    spmm<K, VT, X>(ctx, A, x, MRestrict<K, R, S>{rin, rts_, bs, p}, true);
-    spmm<K, VT, S>(ctx, &P->loc.FL, rts_, MStore<K, S>{tl_});
-    spmm<K, VT, S>(ctx, &P->loc.FUt, tl_, MProlong<K, X>{x, bs, p});
+    spmm<K, VT, R>(ctx, &P->glo.FL, rin, MStore<K, S>{tg_}, false, gate);
+    spmm<K, VT, S>(ctx, &P->glo.FUt, tg_, MStore<K, X>{x}, false, gate);
+    spmm<K, VT, X>(ctx, A, x, MRestrict<K, R, S>{rin, rts_, bs, p}, true, gate);
+    spmm<K, VT, S>(ctx, &P->loc.FL, rts_, MStore<K, S>{tl_}, false, gate);
+    spmm<K, VT, S>(ctx, &P->loc.FUt, tl_, MProlong<K, X>{x, bs, p}, false, gate);
     if (P->prm.seq == 0) return;
-    spmm<K, VT, X>(ctx, A, x, MResid<K, R, S>{rin, rt_});
-    spmm<K, VT, S>(ctx, &P->glo.FL, rt_, MStore<K, S>{tg_});
-    spmm<K, VT, S>(ctx, &P->glo.FUt, tg_, MAdd<K, X>{x});
+    spmm<K, VT, X>(ctx, A, x, MResid<K, R, S>{rin, rt_}, false, gate);
+    spmm<K, VT, S>(ctx, &P->glo.FL, rt_, MStore<K, S>{tg_}, false, gate);
+    spmm<K, VT, S>(ctx, &P->glo.FUt, tg_, MAdd<K, X>{x}, false, gate);
   }
+
+  MMGate inner_gate() const { return MMGate{B->cell_sys.get(), in.sys_active, B->ncell, 1}; }
 
   template <typename R, typename X>
   void apply_inner(const R* rin, X* x) {
-    if constexpr (sizeof(T) == 4) precond<float>(rin, x, tg.get(), tl.get(), rt.get(), rts.get());
-    else precond<double>(rin, x, tg.get(), tl.get(), rt.get(), rts.get());
+    if constexpr (sizeof(T) == 4) precond<float>(rin, x, tg.get(), tl.get(), rt.get(), rts.get(), inner_gate());
+    else precond<double>(rin, x, tg.get(), tl.get(), rt.get(), rts.get(), inner_gate());
   }
 
   void apply_outer(const double* rin, double* x) {
@@ -601,10 +615,10 @@ struct BatchSolver {
       apply_inner<T, T>(col(j), z.get());
       if constexpr (sizeof(T) == 4)
         spmm<K, float, T>(ctx, B->A, z.get(), MStoreScaled<K, T>{w.get(), st.base + soff + j, st.stride,
-                                                                  B->cell_sys.get(), B->bs});
+                                                                  B->cell_sys.get(), B->bs}, false, inner_gate());
       else
         spmm<K, double, T>(ctx, B->A, z.get(), MStoreScaled<K, T>{w.get(), st.base + soff + j, st.stride,
-                                                                   B->cell_sys.get(), B->bs});
+                                                                   B->cell_sys.get(), B->bs}, false, inner_gate());
       const int ngroups = (j + 1 + kGroup - 1) / kGroup;
       b_dots<K, T><<<dim3(nch, ngroups), kT, 0, s>>>(crow, csys, in, ld, j, V.get(), w.get(), red.get(), nch);
       DECO_CHECK_LAUNCH();
@@ -646,36 +660,73 @@ struct BatchSolver {
     DECO_CHECK_LAUNCH();
     DECO_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * (size_t)nk, s));
     DECO_CUDA(cudaMemcpyAsync(r.get(), bdec.get(), sizeof(double) * (size_t)nk, cudaMemcpyDeviceToDevice, s));
-    // the cycle as a CUDA graph, captured once and replayed
+    // Cycle launch mode (DECO_BATCH_GRAPH): 2 (default) the whole solve is ONE
+    // graph launch, the cycle graph inside a device-side while loop (a conditional
+    // graph node whose condition the last kernel of the cycle sets from the count
+    // of unfinished instances and a cycle counter bounded by itmax / m + 2);
+    // 1: the cycle graph relaunched by the host, which reads the count after each
+    // cycle; 0: the same kernels launched directly.
+    int mode = 2;
+    if (const char* e = std::getenv("DECO_BATCH_GRAPH")) mode = std::max(0, std::min(2, std::atoi(e)));
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    const bool use_graph = !(std::getenv("DECO_BATCH_GRAPH") && std::atoi(std::getenv("DECO_BATCH_GRAPH")) == 0);
     struct GraphGuard {
       cudaGraph_t* g; cudaGraphExec_t* e;
       ~GraphGuard() { if (*e) cudaGraphExecDestroy(*e); if (*g) cudaGraphDestroy(*g); }
     } gg{&graph, &exec};
-    if (use_graph) {
-      DECO_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const int max_cycles = prm.itmax / std::max(1, m) + 2;
+    DECO_CUDA(cudaMemsetAsync(cyc.get(), 0, sizeof(int), s));
+    auto capture = [&](cudaGraph_t into, bool loop_tail, cudaGraphConditionalHandle h) {
+      if (into) DECO_CUDA(cudaStreamBeginCaptureToGraph(s, into, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+      else DECO_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       try {
         cycle(x);
+        if (loop_tail) {
+          b_continue<<<1, 1, 0, s>>>(h, in.remaining, cyc.get(), max_cycles);
+          DECO_CHECK_LAUNCH();
+        }
       } catch (...) {
         cudaGraph_t tmp = nullptr;
         cudaStreamEndCapture(s, &tmp);
-        if (tmp) cudaGraphDestroy(tmp);
+        if (tmp && !into) cudaGraphDestroy(tmp);
         throw;
       }
-      DECO_CUDA(cudaStreamEndCapture(s, &graph));
+      cudaGraph_t out = nullptr;
+      DECO_CUDA(cudaStreamEndCapture(s, &out));
+      if (!into) graph = out;
+    };
+    if (mode == 2) {
+      DECO_CUDA(cudaGraphCreate(&graph, 0));
+      cudaGraphConditionalHandle h;
+      DECO_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault));
+      cudaGraphNodeParams cp = {};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      cudaGraphNode_t node;
+      DECO_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+      capture(cp.conditional.phGraph_out[0], true, h);
+      DECO_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    } else if (mode == 1) {
+      capture(nullptr, false, 0);
       DECO_CUDA(cudaGraphInstantiate(&exec, graph, 0));
     }
     volatile int* hrem = reinterpret_cast<volatile int*>(ctx->host_scalars + 64);
-    const int max_cycles = prm.itmax / std::max(1, m) + 2;
     int cycles = 0;
-    for (; cycles < max_cycles; ++cycles) {
-      if (use_graph) DECO_CUDA(cudaGraphLaunch(exec, s));
-      else cycle(x);
-      DECO_CUDA(cudaMemcpyAsync(const_cast<int*>(hrem), in.remaining, sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (mode == 2) {
+      DECO_CUDA(cudaGraphLaunch(exec, s));
+      DECO_CUDA(cudaMemcpyAsync(const_cast<int*>(hrem), cyc.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
       DECO_CUDA(cudaStreamSynchronize(s));
-      if (*hrem == 0) { ++cycles; break; }
+      cycles = *hrem;
+    } else {
+      for (; cycles < max_cycles; ++cycles) {
+        if (mode == 1) DECO_CUDA(cudaGraphLaunch(exec, s));
+        else cycle(x);
+        DECO_CUDA(cudaMemcpyAsync(const_cast<int*>(hrem), in.remaining, sizeof(int), cudaMemcpyDeviceToHost, s));
+        DECO_CUDA(cudaStreamSynchronize(s));
+        if (*hrem == 0) { ++cycles; break; }
+      }
     }
     int hb = 0;
     DECO_CUDA(cudaMemcpyAsync(&hb, brk.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -702,7 +753,7 @@ struct BatchSolver {
     res->converged = nconv;
     res->cycles = cycles;
     res->t_solve_ms = ms;
-    res->graph = use_graph ? 1 : 0;
+    res->graph = mode;
   }
 };
 

@@ -16,6 +16,8 @@
 //   class 3 (32 < k <= 64): one warp per row, M in shared memory (32 KB).
 #include <algorithm>
 
+#include <climits>
+
 #include "fsai.cuh"
 
 namespace deco {
@@ -88,6 +90,75 @@ __global__ void lower_copy(int n, const int* __restrict__ r, const int* __restri
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     int o = fr[i];
     for (int j = r[i]; j < r[i + 1] && c[j] <= i; ++j) fc[o++] = c[j];
+  }
+}
+
+// ---------------------------------------------------------- lower(A·A) pattern
+// precond/FSAI/symbolic.tpp:149-172 (power 2): row i of the pattern is the set
+// of columns c <= i of the rows k of A that row i of A references, sorted.
+// One warp per row: the candidates gather into the warp's shared-memory buffer
+// (ballot-compacted), a bitonic sort orders them, and the distinct values are
+// counted (mode 0) or written (mode 1).  A row with more than kSqCap candidates
+// raises *overflow and is left out (the caller reports it).
+constexpr int kSqCap = 2048;
+constexpr int kSqWarps = 4;
+
+__global__ void __launch_bounds__(kSqWarps * 32) lower_square(int n, const int* __restrict__ r,
+                                                             const int* __restrict__ c, int mode,
+                                                             int* __restrict__ cnt, const int* __restrict__ fr,
+                                                             int* __restrict__ fc, int* __restrict__ overflow) {
+  extern __shared__ int sqbuf[];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  int* buf = sqbuf + wl * kSqCap;
+  const unsigned lt = (1u << lane) - 1u;
+  for (int i = blockIdx.x * kSqWarps + wl; i < n; i += gridDim.x * kSqWarps) {
+    int m = 0;
+    bool over = false;
+    for (int e = r[i]; e < r[i + 1] && !over; ++e) {
+      const int k = c[e];
+      const int kb = r[k], ke = r[k + 1];
+      for (int t0 = kb; t0 < ke; t0 += 32) {
+        const int t = t0 + lane;
+        const int col = t < ke ? c[t] : INT_MAX;
+        const bool take = col <= i;
+        const unsigned mask = __ballot_sync(0xffffffffu, take);
+        if (m + __popc(mask) > kSqCap) { over = true; break; }
+        if (take) buf[m + __popc(mask & lt)] = col;
+        m += __popc(mask);
+        // row k is sorted: once a lane sees a column > i, the rest of the row is too
+        if (__any_sync(0xffffffffu, t < ke && col > i)) break;
+      }
+    }
+    if (over) {
+      if (lane == 0) atomicExch(overflow, 1);
+      if (mode == 0 && lane == 0) cnt[i] = 0;
+      continue;
+    }
+    int np2 = 1;
+    while (np2 < m) np2 <<= 1;
+    for (int t = m + lane; t < np2; t += 32) buf[t] = INT_MAX;
+    __syncwarp();
+    for (int size = 2; size <= np2; size <<= 1)
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int t = lane; t < np2 / 2; t += 32) {
+          const int lo = 2 * stride * (t / stride) + (t % stride), hi = lo + stride;
+          const bool up = (lo & size) == 0;
+          const int a = buf[lo], b2 = buf[hi];
+          if ((a > b2) == up) { buf[lo] = b2; buf[hi] = a; }
+        }
+        __syncwarp();
+      }
+    // distinct values, in order
+    int total = 0;
+    for (int t0 = 0; t0 < m; t0 += 32) {
+      const int t = t0 + lane;
+      const bool first = t < m && (t == 0 || buf[t] != buf[t - 1]);
+      const unsigned mask = __ballot_sync(0xffffffffu, first);
+      if (mode == 1 && first) fc[fr[i] + total + __popc(mask & lt)] = buf[t];
+      total += __popc(mask);
+    }
+    if (mode == 0 && lane == 0) cnt[i] = total;
+    __syncwarp();
   }
 }
 
@@ -544,7 +615,8 @@ void fsai_build(deco_ctx_s* ctx, const deco_csr_s* A0, double tol_rel, double to
                 deco_fsai_s* F, int bs) {
   cudaStream_t st = ctx->stream;
   DECO_REQUIRE(A0->n == A0->m, DECO_ERR_ARG, "FSAI needs a square matrix");
-  DECO_REQUIRE(power == 1, DECO_ERR_UNSUPPORTED, "FSAI power 2 (lower(A^2) pattern) is not available on the GPU path");
+  DECO_REQUIRE(power == 1 || power == 2, DECO_ERR_UNSUPPORTED,
+               "FSAI power " + std::to_string(power) + " is not implemented (symbolic.tpp:173-176 supports 1 and 2)");
   DECO_REQUIRE(precision == 64 || precision == 32, DECO_ERR_ARG, "precision must be 64 or 32");
   const int n = A0->n;
   trace_mark(ctx, nullptr);
@@ -559,19 +631,40 @@ void fsai_build(deco_ctx_s* ctx, const deco_csr_s* A0, double tol_rel, double to
   }
   const int g = grid_for(ctx, n, 256);
   trace_mark(ctx, "fsai filter");
-  // 2. symbolic: lower(A)
+  // 2. symbolic: lower(A) (power 1) or lower(A A) (power 2)
   DevBuf<int> cnt(n + 1, st);
-  lower_count<<<g, 256, 0, st>>>(n, A->r.get(), A->c.get(), cnt.get());
-  DECO_CHECK_LAUNCH();
   deco_csr_s& FL = F->FL;
   FL.n = FL.m = n;
   FL.r.alloc(n + 1, st);
-  FL.nz = (int)exclusive_scan_int(ctx, cnt.get(), FL.r.get(), n);
-  FL.c.alloc(FL.nz, st);
+  if (power == 1) {
+    lower_count<<<g, 256, 0, st>>>(n, A->r.get(), A->c.get(), cnt.get());
+    DECO_CHECK_LAUNCH();
+    FL.nz = (int)exclusive_scan_int(ctx, cnt.get(), FL.r.get(), n);
+    FL.c.alloc(FL.nz, st);
+    lower_copy<<<g, 256, 0, st>>>(n, A->r.get(), A->c.get(), FL.r.get(), FL.c.get());
+    DECO_CHECK_LAUNCH();
+  } else {
+    const size_t smem = sizeof(int) * kSqCap * kSqWarps;
+    DECO_CUDA(cudaFuncSetAttribute(lower_square, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    DevBuf<int> over(1, st);
+    over.zero(st);
+    const int gs = grid_for(ctx, cdiv(n, kSqWarps), 1, 16);
+    lower_square<<<gs, kSqWarps * 32, smem, st>>>(n, A->r.get(), A->c.get(), 0, cnt.get(), nullptr, nullptr,
+                                                  over.get());
+    DECO_CHECK_LAUNCH();
+    FL.nz = (int)exclusive_scan_int(ctx, cnt.get(), FL.r.get(), n);
+    int ho = 0;
+    DECO_CUDA(cudaMemcpyAsync(&ho, over.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+    DECO_CUDA(cudaStreamSynchronize(st));
+    DECO_REQUIRE(ho == 0, DECO_ERR_UNSUPPORTED,
+                 "FSAI power 2: a row of A A has more than " + std::to_string(kSqCap) + " candidate columns");
+    FL.c.alloc(FL.nz, st);
+    lower_square<<<gs, kSqWarps * 32, smem, st>>>(n, A->r.get(), A->c.get(), 1, nullptr, FL.r.get(), FL.c.get(),
+                                                  over.get());
+    DECO_CHECK_LAUNCH();
+  }
   FL.v.alloc(FL.nz, st);
   FL.v.zero(st);
-  lower_copy<<<g, 256, 0, st>>>(n, A->r.get(), A->c.get(), FL.r.get(), FL.c.get());
-  DECO_CHECK_LAUNCH();
   F->nz = FL.nz;
   DevBuf<double> fu(FL.nz, st);  // FU values in FL's (lower) layout before the transpose
   fu.zero(st);

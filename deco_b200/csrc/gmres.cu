@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <type_traits>
 #include <vector>
 
 #include "cpr.cuh"
@@ -69,14 +70,26 @@ struct State {
 enum { SC_RES = 0, SC_BREAK = 1, SC_BETA = 2 };
 
 
-// deterministic last-block reduction of red[i*nb + b] over b for i < ncols
+// deterministic last-block reduction of red[i*nb + b] over b for i < ncols.
+// Warp w owns columns w, w + 8, ...; it works on four of them at once so four
+// independent loads per lane are in flight (this runs in one block while the
+// rest of the GPU waits); each column's summation order is the lane-strided one.
 __device__ void finalize_partials(const double* red, int nb, int ncols, double* out) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int i = warp; i < ncols; i += kWarps) {
-    double s = 0.0;
-    for (int b = lane; b < nb; b += 32) s += __ldcg(red + (size_t)i * nb + b);
-    s = warp_sum(s);
-    if (lane == 0) out[i] = s;
+  for (int i0 = warp; i0 < ncols; i0 += 4 * kWarps) {
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    const double* p[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) p[u] = red + (size_t)min(i0 + u * kWarps, ncols - 1) * nb;
+#pragma unroll 4
+    for (int b = lane; b < nb; b += 32)
+#pragma unroll
+      for (int u = 0; u < 4; ++u) s[u] += __ldcg(p[u] + b);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const double t = warp_sum(s[u]);
+      if (lane == 0 && i0 + u * kWarps < ncols) out[i0 + u * kWarps] = t;
+    }
   }
 }
 
@@ -133,12 +146,40 @@ template <> struct Vec4<double> {
   __device__ static double get(const double2& a, int e) { return e == 0 ? a.x : a.y; }
 };
 
-// ---- pass A: raw dots u_c . w and u_c . u_j for c < ncols (u = stored columns).
-// Blocks own contiguous ranges of 128-bit vectors; warp w owns columns w, w+8, ...;
-// lanes keep per-column partial sums in registers for the whole range (no
-// barriers).  Rows past the last full vector are summed by the last block.
+// last block of pass A: h, the new Gram row, c = h + (h - G h) and H(:,j)
+__device__ void dots_finish(int ncols, int j, const double* __restrict__ red, State st) {
+  finalize_partials(red, gridDim.x, 2 * ncols, st.sums);
+  __syncthreads();
+  // h_i = s_i (u_i . w);  G(i,j) = s_i s_j (u_i . u_j)
+  __shared__ double hs[kMaxCols];
+  const double sj = st.s[j];
+  for (int i = threadIdx.x; i < ncols; i += kThreads) {
+    hs[i] = st.sums[i] * st.s[i];
+    const double gij = st.s[i] * sj * st.sums[ncols + i];
+    st.gm(i, j) = gij;
+    st.gm(j, i) = gij;
+  }
+  __syncthreads();
+  // c = h + (h - G h): the second Gram-Schmidt projection from the Gram matrix
+  // (one thread per row of G; the loads of a row are independent, so several
+  // are in flight while the sum runs in order)
+  for (int i = threadIdx.x; i < ncols; i += kThreads) {
+    double gh = 0.0;
+#pragma unroll 8
+    for (int k = 0; k < ncols; ++k) gh += st.gm(i, k) * hs[k];
+    const double ci = hs[i] + (hs[i] - gh);
+    st.h(i, j) = ci;
+    st.c[i] = ci * st.s[i];  // coefficient on the stored (unnormalised) column
+  }
+}
+
+
+// ---- pass A for a float64 basis: the same dots, warp w owning columns w, w+8, ...
+// over the block's range of 128-bit vectors, partial sums in registers for the
+// whole range (no barriers; with double2 loads the grouped sweep below needs too
+// many registers).  Rows past the last full vector are summed by the last block.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long ld, int ncols, int j,
+__global__ void __launch_bounds__(kThreads) arnoldi_dots_cols(long long n, long long ld, int ncols, int j,
                                                          const T* __restrict__ V, const T* __restrict__ w,
                                                          double* __restrict__ red, unsigned* counter, State st) {
   using VT = typename Vec4<T>::t;
@@ -203,26 +244,72 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long 
     }
   }
   if (!last_block(counter)) return;
-  finalize_partials(red, gridDim.x, 2 * ncols, st.sums);
-  __syncthreads();
-  // h_i = s_i (u_i . w);  G(i,j) = s_i s_j (u_i . u_j)
-  double* h = st.sums;  // scaled in place
-  const double sj = st.s[j];
-  for (int i = threadIdx.x; i < ncols; i += kThreads) {
-    h[i] *= st.s[i];
-    const double gij = st.s[i] * sj * st.sums[ncols + i];
-    st.gm(i, j) = gij;
-    st.gm(j, i) = gij;
+  dots_finish(ncols, j, red, st);
+}
+
+// ---- pass A: raw dots u_c . w and u_c . u_j for c < ncols (u = stored columns).
+// Blocks own contiguous ranges of 128-bit vectors and sweep them once per group
+// of kDotGroup columns: every thread takes one vector of the range per step and
+// keeps 2 kDotGroup partial sums, so each step has kDotGroup independent column
+// loads in flight and every column is read once, fully coalesced; w and u_j are
+// re-read per group from L1/L2.  Partials are reduced per block in a fixed order.
+// Rows past the last full vector are summed by the last block.
+constexpr int kDotGroup = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long ld, int ncols, int j,
+                                                         const T* __restrict__ V, const T* __restrict__ w,
+                                                         double* __restrict__ red, unsigned* counter, State st) {
+  using VT = typename Vec4<T>::t;
+  constexpr int N = Vec4<T>::N;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long nvec = n / N;
+  const long long per = (nvec + gridDim.x - 1) / gridDim.x;
+  const long long v0 = per * blockIdx.x, v1 = min(nvec, v0 + per);
+  const VT* __restrict__ wv4 = reinterpret_cast<const VT*>(w);
+  const VT* __restrict__ uv4 = reinterpret_cast<const VT*>(V + (size_t)j * ld);
+  __shared__ double part[kWarps][2 * kDotGroup];
+  for (int g0 = 0; g0 < ncols; g0 += kDotGroup) {
+    double pw[kDotGroup], pu[kDotGroup];
+#pragma unroll
+    for (int k = 0; k < kDotGroup; ++k) { pw[k] = 0.0; pu[k] = 0.0; }
+    for (long long vi = v0 + threadIdx.x; vi < v1; vi += kThreads) {
+      const VT a = wv4[vi], b = uv4[vi];
+#pragma unroll
+      for (int k = 0; k < kDotGroup; ++k) {
+        const int c = min(g0 + k, ncols - 1);  // clamped: the extra sums are discarded
+        const VT v = __ldcs(reinterpret_cast<const VT*>(V + (size_t)c * ld) + vi);
+        pw[k] += Vec4<T>::dot(v, a);
+        pu[k] += Vec4<T>::dot(v, b);
+      }
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {  // rows past the last full vector
+      const T* __restrict__ uj = V + (size_t)j * ld;
+      for (long long r = nvec * N; r < n; ++r)
+#pragma unroll
+        for (int k = 0; k < kDotGroup; ++k) {
+          const double v = (double)V[(size_t)min(g0 + k, ncols - 1) * ld + r];
+          pw[k] += v * (double)w[r];
+          pu[k] += v * (double)uj[r];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kDotGroup; ++k) {
+      const double a = warp_sum(pw[k]), b = warp_sum(pu[k]);
+      if (lane == 0) { part[warp][k] = a; part[warp][kDotGroup + k] = b; }
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * kDotGroup) {
+      const int k = threadIdx.x % kDotGroup, c = g0 + k;
+      double t = 0.0;
+#pragma unroll
+      for (int q = 0; q < kWarps; ++q) t += part[q][threadIdx.x];
+      if (c < ncols) red[(size_t)(threadIdx.x < kDotGroup ? c : ncols + c) * gridDim.x + blockIdx.x] = t;
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  // c = h + (h - G h): the second Gram-Schmidt projection from the Gram matrix
-  for (int i = threadIdx.x; i < ncols; i += kThreads) {
-    double gh = 0.0;
-    for (int k = 0; k < ncols; ++k) gh += st.gm(i, k) * h[k];
-    const double ci = h[i] + (h[i] - gh);
-    st.h(i, j) = ci;
-    st.c[i] = ci * st.s[i];  // coefficient on the stored (unnormalised) column
-  }
+  if (!last_block(counter)) return;
+  dots_finish(ncols, j, red, st);
 }
 
 // ---- pass B: w'' = w - sum_c coef_c u_c, stored as column j+1; ||w''||^2.
@@ -276,17 +363,24 @@ __global__ void __launch_bounds__(kThreads) arnoldi_update(long long n, long lon
   block_sum_to(ss, red + blockIdx.x);
   if (!last_block(counter)) return;
   finalize_partials(red, gridDim.x, 1, st.sc + SC_BETA);
+  // the rotations run on a shared-memory copy of column j and of the earlier
+  // rotations (one thread, a chain of j dependent updates)
+  __shared__ double hc[kMaxCols + 1], rc[kMaxCols], rs[kMaxCols];
+  for (int i = threadIdx.x; i <= j; i += kThreads) hc[i] = st.h(i, j);
+  for (int i = threadIdx.x; i < j; i += kThreads) { rc[i] = st.cs[i]; rs[i] = st.sn[i]; }
   __syncthreads();
   if (threadIdx.x == 0) {
     const double beta = sqrt(st.sc[SC_BETA]);
-    st.h(j + 1, j) = beta;
+    hc[j + 1] = beta;
     st.s[j + 1] = beta != 0.0 ? 1.0 / beta : 0.0;
-    for (int i = 0; i <= j - 1; ++i) givens_apply(st.cs[i], st.sn[i], st.h(i, j), st.h(i + 1, j));
-    givens_make(st.h(j, j), st.h(j + 1, j), st.cs[j], st.sn[j]);
-    givens_apply(st.cs[j], st.sn[j], st.h(j, j), st.h(j + 1, j));
+    for (int i = 0; i <= j - 1; ++i) givens_apply(rc[i], rs[i], hc[i], hc[i + 1]);
+    givens_make(hc[j], hc[j + 1], st.cs[j], st.sn[j]);
+    givens_apply(st.cs[j], st.sn[j], hc[j], hc[j + 1]);
     givens_apply(st.cs[j], st.sn[j], st.g[j], st.g[j + 1]);
     st.sc[SC_RES] = fabs(st.g[j + 1]);
   }
+  __syncthreads();
+  for (int i = threadIdx.x; i <= j + 1; i += kThreads) st.h(i, j) = hc[i];
 }
 
 // ---- column 0: u_0 = r, s_0 = 1/||r||, g_0 = ||r|| (rgmres.tpp:54-55); out[0] = ||r||
@@ -379,6 +473,7 @@ struct Solver {
   const deco_sol_params& prm;
   long long n, ld;
   int m, nb;
+  int nb_dots;  // pass A grid: exactly the blocks that fit on the GPU at once (one wave)
   DevBuf<T> V, w, z;
   DevBuf<double> st_buf, xtmp, r64, norm;
   State st{};
@@ -397,6 +492,14 @@ struct Solver {
     ld = (n + 31) / 32 * 32;
     m = prm.restart;
     nb = 4 * ctx->num_sms;
+    {
+      int per_sm = 0;
+      if constexpr (std::is_same<T, float>::value)
+        DECO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, arnoldi_dots<float>, kThreads, 0));
+      else
+        DECO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, arnoldi_dots_cols<double>, kThreads, 0));
+      nb_dots = std::max(1, std::min(nb, per_sm * ctx->num_sms));
+    }
     cudaStream_t s = ctx->stream;
     V.alloc((size_t)ld * (m + 1), s);
     w.alloc(n, s);
@@ -487,7 +590,12 @@ struct Solver {
     }
     if (profile) DECO_CUDA(cudaEventRecord(pev[4 * j + 2], s));
     const int nc = j + 1;
-    arnoldi_dots<T><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V.get(), w.get(), ctx->red.get(), ctx->counter.get(), st);
+    if constexpr (std::is_same<T, float>::value)
+      arnoldi_dots<T><<<nb_dots, kThreads, 0, s>>>(n, ld, nc, j, V.get(), w.get(), ctx->red.get(), ctx->counter.get(),
+                                                   st);
+    else
+      arnoldi_dots_cols<T><<<nb_dots, kThreads, 0, s>>>(n, ld, nc, j, V.get(), w.get(), ctx->red.get(), ctx->counter.get(),
+                                                   st);
     DECO_CHECK_LAUNCH();
     arnoldi_update<T><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V.get(), w.get(), col(j + 1), ctx->red.get(),
                                               ctx->counter.get(), st);

@@ -78,16 +78,25 @@ __device__ __forceinline__ void load_k(const XT* __restrict__ x, long long o, do
   }
 }
 
+// Optional skip of finished systems: block row s is left out (its outputs are
+// not written) when active[cell_sys[s / div]] == 0.
+struct MMGate {
+  const int* cell_sys = nullptr;
+  const int* active = nullptr;
+  int ncell = 0;  // cells of the system the map covers
+  int div = 1;    // block rows per cell of the matrix at hand (set by spmm)
+};
+
 // ------------------------------------------------------------ the kernel
 template <int SW, int BS, int K, bool ROW0, typename VT, typename XT, class Epi>
 __global__ void __launch_bounds__(256) bsr_mm_kernel(int nbr, const int* __restrict__ br, const int* __restrict__ bc,
                                                      const VT* __restrict__ bv, long long plane,
-                                                     const XT* __restrict__ x, Epi epi) {
+                                                     const XT* __restrict__ x, Epi epi, MMGate gate) {
   constexpr int NR = ROW0 ? 1 : BS;
   const int lane = threadIdx.x & (SW - 1);
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int s = int(gid / SW);
-  const bool valid = s < nbr;
+  const bool valid = s < nbr && (!gate.active || __ldg(gate.active + __ldg(gate.cell_sys + s / gate.div)) != 0);
   double acc[NR][K];
 #pragma unroll
   for (int q = 0; q < NR; ++q)
@@ -153,41 +162,46 @@ inline MMView mm_view(const deco_csr_s* A) {
 }
 
 template <int SW, int BS, int K, bool ROW0, typename VT, typename XT, class Epi>
-void launch_mm_sw(cudaStream_t st, const MMView& M, const VT* v, const XT* x, Epi epi) {
+void launch_mm_sw(cudaStream_t st, const MMView& M, const VT* v, const XT* x, Epi epi, MMGate gate) {
   const unsigned grid = (unsigned)cdiv((long long)M.nbr * SW, 256);
-  bsr_mm_kernel<SW, BS, K, ROW0, VT, XT, Epi><<<grid, 256, 0, st>>>(M.nbr, M.br, M.bc, v, M.plane, x, epi);
+  bsr_mm_kernel<SW, BS, K, ROW0, VT, XT, Epi><<<grid, 256, 0, st>>>(M.nbr, M.br, M.bc, v, M.plane, x, epi, gate);
   DECO_CHECK_LAUNCH();
 }
 
 template <int BS, int K, bool ROW0, typename VT, typename XT, class Epi>
-void launch_mm_bs(cudaStream_t st, const MMView& M, const VT* v, const XT* x, Epi epi) {
+void launch_mm_bs(cudaStream_t st, const MMView& M, const VT* v, const XT* x, Epi epi, MMGate gate) {
   switch (M.sw) {
-    case 1: launch_mm_sw<1, BS, K, ROW0>(st, M, v, x, epi); break;
-    case 2: launch_mm_sw<2, BS, K, ROW0>(st, M, v, x, epi); break;
-    case 4: launch_mm_sw<4, BS, K, ROW0>(st, M, v, x, epi); break;
-    case 8: launch_mm_sw<8, BS, K, ROW0>(st, M, v, x, epi); break;
-    default: launch_mm_sw<16, BS, K, ROW0>(st, M, v, x, epi); break;
+    case 1: launch_mm_sw<1, BS, K, ROW0>(st, M, v, x, epi, gate); break;
+    case 2: launch_mm_sw<2, BS, K, ROW0>(st, M, v, x, epi, gate); break;
+    case 4: launch_mm_sw<4, BS, K, ROW0>(st, M, v, x, epi, gate); break;
+    case 8: launch_mm_sw<8, BS, K, ROW0>(st, M, v, x, epi, gate); break;
+    default: launch_mm_sw<16, BS, K, ROW0>(st, M, v, x, epi, gate); break;
   }
 }
 
 // Y = op(A X) with K columns; row0: the restricted product over row 0 of every
 // cell of size `bs` (A must then have a cell-block copy of that size, or bs = 1).
 template <int K, typename VT, typename XT, class Epi>
-void spmm(deco_ctx_s* ctx, const deco_csr_s* A, const XT* x, Epi epi, bool row0 = false, int sw = 0) {
+void spmm(deco_ctx_s* ctx, const deco_csr_s* A, const XT* x, Epi epi, bool row0 = false, MMGate gate = MMGate{},
+          int sw = 0) {
   MMView M = mm_view(A);
   if (sw) M.sw = sw;
   const VT* v;
   if constexpr (sizeof(VT) == 4) v = M.v32; else v = M.v64;
   DECO_REQUIRE(v != nullptr, DECO_ERR_INTERNAL, "matrix values of the requested precision are missing");
   DECO_REQUIRE(!row0 || M.bs > 1, DECO_ERR_INTERNAL, "restricted K-column product needs a cell-block copy");
+  if (gate.active) {  // block rows per cell: 1 for cell blocks and the pressure system, bs for scalar rows
+    if (gate.ncell > 0 && M.nbr % gate.ncell == 0) gate.div = M.nbr / gate.ncell;
+    else gate = MMGate{};
+  }
   cudaStream_t st = ctx->stream;
-  if (M.bs == 1) launch_mm_bs<1, K, false, VT, XT, Epi>(st, M, v, x, epi);
+  if (M.bs == 1) launch_mm_bs<1, K, false, VT, XT, Epi>(st, M, v, x, epi, gate);
   else if (M.bs == 2) {
-    if (row0) launch_mm_bs<2, K, true, VT, XT, Epi>(st, M, v, x, epi);
-    else launch_mm_bs<2, K, false, VT, XT, Epi>(st, M, v, x, epi);
+    if (row0) launch_mm_bs<2, K, true, VT, XT, Epi>(st, M, v, x, epi, gate);
+    else launch_mm_bs<2, K, false, VT, XT, Epi>(st, M, v, x, epi, gate);
   } else {
-    if (row0) launch_mm_bs<3, K, true, VT, XT, Epi>(st, M, v, x, epi);
-    else launch_mm_bs<3, K, false, VT, XT, Epi>(st, M, v, x, epi);
+    if (row0) launch_mm_bs<3, K, true, VT, XT, Epi>(st, M, v, x, epi, gate);
+    else launch_mm_bs<3, K, false, VT, XT, Epi>(st, M, v, x, epi, gate);
   }
 }
 

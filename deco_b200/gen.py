@@ -170,3 +170,23 @@ def batch(nsys: int = 64, seed: int = 1234, cells_lo: int = 10_000, cells_hi: in
     n = int(row_off[-1])
     B = uniform(seed, 913, n * nrhs)
     return r, c, v, row_off, B, shapes
+
+
+def batch_subset(r, c, v, row_off, B, nrhs: int, systems):
+    """The block-diagonal matrix and right-hand sides of the listed systems of a batch
+    (e.g. one rank's share when independent systems are spread over GPUs)."""
+    rs, cs, vs, offs, bs_ = [], [], [], [0], []
+    nz_off = 0
+    Bm = np.asarray(B).reshape(-1, nrhs)
+    for q in systems:
+        a, e = int(row_off[q]), int(row_off[q + 1])
+        ra, re = int(r[a]), int(r[e])
+        rs.append((r[a:e] - ra + nz_off).astype(np.int64))
+        cs.append(c[ra:re] - a + offs[-1])
+        vs.append(v[ra:re])
+        bs_.append(Bm[a:e])
+        nz_off += re - ra
+        offs.append(offs[-1] + (e - a))
+    r2 = np.concatenate(rs + [np.array([nz_off], np.int64)]).astype(np.int32)
+    return (r2, np.concatenate(cs).astype(np.int32), np.concatenate(vs), np.array(offs, np.int32),
+            np.ascontiguousarray(np.concatenate(bs_).reshape(-1)))

@@ -7,6 +7,8 @@
 // r[n+1]; c[nz]; v[nz] and int n; b[n]; rhs "ones" = A*1), builds
 // CPR<int,int,double,FSAI,FSAI> and SOL on the GPU and prints the reference's
 // solver summary (rgmres.tpp:130-135) and its profiler node names.
+// prec.row_order / prec.col_order other than 12(3) reorder every cell's unknowns
+// first, as the reference's driver does (cpr.cpp:41, adapter/csr2coo.cpp).
 // `"parallel": {"hardware": "GPU"}` selects this path; the reference never reads
 // that key (cpr.cpp:19-21).  IO.format "synthetic" (IO.preset, IO.seed) runs a
 // generated system instead of files.
@@ -69,6 +71,50 @@ static bool read_rhs(const std::string& fn, int n, const std::vector<int>& r, co
   return (bool)f;
 }
 
+// AD::block_reorder (adapter/csr2coo.cpp:18-86): the unknowns of every cell are
+// permuted so the pressure equation and variable come first.  row_order /
+// col_order list, for each new position, the old 1-based position in the cell.
+// New row s*bs + p is old row s*bs + (row_order[p] - 1); each column moves
+// within its cell the same way by col_order; rows end up sorted by column (the
+// reference sorts the coordinate list by row, then column) and b follows the rows.
+static void block_reorder(int n, std::vector<int>& r, std::vector<int>& c, std::vector<double>& v,
+                          std::vector<double>& b, int bs, const std::string& row_order, const std::string& col_order) {
+  if ((int)row_order.size() != bs || (int)col_order.size() != bs)
+    throw std::invalid_argument("prec.row_order / prec.col_order must list the " + std::to_string(bs) +
+                                " positions of a cell");
+  std::vector<int> ord_row(bs), reord_col(bs);
+  for (int i = 0; i < bs; ++i) {
+    const int ro = row_order[i] - '1', co = col_order[i] - '1';
+    if (ro < 0 || ro >= bs || co < 0 || co >= bs) throw std::invalid_argument("bad prec.row_order / prec.col_order");
+    ord_row[i] = ro;
+    reord_col[co] = i;
+  }
+  std::vector<int> nr(n + 1, 0), nc(c.size());
+  std::vector<double> nv(v.size()), nb(b.size());
+  for (int i = 0; i < n; ++i) {
+    const int old = i - i % bs + ord_row[i % bs];
+    nr[i + 1] = nr[i] + (r[old + 1] - r[old]);
+  }
+  std::vector<std::pair<int, double>> row;
+  for (int i = 0; i < n; ++i) {
+    const int old = i - i % bs + ord_row[i % bs];
+    row.clear();
+    for (int j = r[old]; j < r[old + 1]; ++j) row.emplace_back(c[j] - c[j] % bs + reord_col[c[j] % bs], v[j]);
+    std::sort(row.begin(), row.end(), [](const std::pair<int, double>& a, const std::pair<int, double>& b) {
+      return a.first < b.first;
+    });
+    for (size_t k = 0; k < row.size(); ++k) {
+      nc[nr[i] + k] = row[k].first;
+      nv[nr[i] + k] = row[k].second;
+    }
+    nb[i] = b[old];
+  }
+  r.swap(nr);
+  c.swap(nc);
+  v.swap(nv);
+  b.swap(nb);
+}
+
 int main(int argc, char** argv) {
   if (argc < 2) {
     std::cerr << "Usage: " << argv[0] << " param.json [--precision 64|32]" << std::endl;
@@ -109,14 +155,11 @@ int main(int argc, char** argv) {
       throw std::invalid_argument("Unknown global IO::format: " + format);
     }
     const int bs = param.get<int>("prec.block_size");
-    for (const char* key : {"prec.row_order", "prec.col_order"}) {
-      std::string ord = param.get<std::string>(key, "");
+    {
       std::string id;
       for (int k = 1; k <= bs; ++k) id += char('0' + k);
-      if (!ord.empty() && ord != id)
-        throw gpu_error(DECO_ERR_UNSUPPORTED, std::string(key) + " = " + ord +
-                                                  ": block reordering (adapter/csr2coo.cpp) is not on the GPU path; "
-                                                  "supply pressure-first systems");
+      const std::string ro = param.get<std::string>("prec.row_order", id), co = param.get<std::string>("prec.col_order", id);
+      if (ro != id || co != id) block_reorder(n, r, c, v, b, bs, ro, co);
     }
     std::printf("matrix size:\tn = %d, m = %d, nz = %d  (IO %.3f s)\n", n, m, nz, now() - t0);
 

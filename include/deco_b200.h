@@ -279,7 +279,8 @@ typedef struct deco_batch_result {
   int max_iter;          /* largest inner iteration count over the instances  */
   int converged;         /* instances with flag 0                             */
   int cycles;            /* restart cycles run                                */
-  int graph;             /* 1: the cycles ran as a captured CUDA graph        */
+  int graph;             /* 2: one graph launch with a device-side cycle loop;
+                            1: the cycle graph relaunched per cycle; 0: direct */
   double t_solve_ms;     /* device time of the solve                          */
 } deco_batch_result;
 

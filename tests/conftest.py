@@ -25,11 +25,12 @@ def _built():
 
 
 def cpr_json(bs, seq=3, drs=0, weights="quasiimpes_GE", glo_rel=0.0, glo_abs=1e-16, loc_rel=1e-4, loc_abs=1e-16,
-             tol_zero=0.0, cpd=1, e_ps=0.0, glo="FSAI", loc="FSAI", glo_bs=None, loc_bs=None):
+             tol_zero=0.0, cpd=1, e_ps=0.0, glo="FSAI", loc="FSAI", glo_bs=None, loc_bs=None, glo_power=1,
+             loc_power=1):
     """A `prec` object in the reference's parameter-file layout (precond/CPR.hpp:49-65,118,130);
     glo/loc "Jacobi" select Jacobi stages, glo_bs/loc_bs their block_size (Jacobi.hpp:21)."""
-    g = {"type": glo, "tol_rel": str(glo_rel), "tol_abs": str(glo_abs), "power": "1"}
-    l = {"type": loc, "tol_rel": str(loc_rel), "tol_abs": str(loc_abs), "power": "1"}
+    g = {"type": glo, "tol_rel": str(glo_rel), "tol_abs": str(glo_abs), "power": str(glo_power)}
+    l = {"type": loc, "tol_rel": str(loc_rel), "tol_abs": str(loc_abs), "power": str(loc_power)}
     if glo_bs is not None or seq == 2 or glo == "Jacobi":
         g["block_size"] = str(glo_bs if glo_bs is not None else bs)
     if loc_bs is not None or loc == "Jacobi":

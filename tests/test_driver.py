@@ -104,3 +104,41 @@ def test_driver_adjoint_section(tmp_path):
     lam = np.frombuffer(raw[4:].tobytes(), np.float64)
     lam_ref = adjoint.adjoint(prec, sol, s.r, s.c, s.v, g, "port")["x"]
     assert np.linalg.norm(lam - lam_ref) / np.linalg.norm(lam_ref) < 1e-7
+
+
+@pytest.mark.gpu
+def test_driver_block_reorder(tmp_path):
+    """prec.row_order / col_order "21" (adapter/csr2coo.cpp:18-86): a system stored
+    saturation-first is reordered pressure-first by the driver and solves like the
+    pressure-first original."""
+    from deco_b200 import gen
+    from oracle import port
+    s = gen.grid(10, 8, 5, bs=2, seed=4)
+    rows = np.repeat(np.arange(s.n), np.diff(s.r))
+    swap = lambda i: i - i % 2 + (1 - i % 2)
+    # scrambled copy: row i of it is original row swap(i), columns swapped within cells
+    perm_rows = swap(np.arange(s.n))
+    r2 = np.zeros(s.n + 1, np.int32)
+    np.cumsum(np.diff(s.r)[perm_rows], out=r2[1:])
+    c2, v2 = np.empty_like(s.c), np.empty_like(s.v)
+    for i in range(s.n):
+        a, e = s.r[perm_rows[i]], s.r[perm_rows[i] + 1]
+        cc, vv = swap(s.c[a:e]), s.v[a:e]
+        o = np.argsort(cc, kind="stable")
+        c2[r2[i]:r2[i + 1]], v2[r2[i]:r2[i + 1]] = cc[o], vv[o]
+    b2 = s.b[perm_rows]
+    fa, fb = tmp_path / "A.bin", tmp_path / "b.bin"
+    with open(fa, "wb") as f:
+        np.array([s.n, s.n, s.nnz], np.int32).tofile(f)
+        r2.tofile(f); c2.astype(np.int32).tofile(f); v2.tofile(f)
+    with open(fb, "wb") as f:
+        np.array([s.n], np.int32).tofile(f)
+        b2.tofile(f)
+    prec = dict(cpr_json(2), row_order="21", col_order="21")
+    sol = sol_json()
+    io = {"file_A": str(fa), "file_b": str(fb), "format": "bin", "wfile_x": str(tmp_path / "x.bin")}
+    rc, it, res, out = run(write_params(tmp_path, io, prec, sol))
+    assert rc == 0, out.stderr
+    ref_it = port.Cpr(cpr_json(2), s.r, s.c, s.v, s.b).solve(sol)["iter"]
+    assert abs(it - ref_it) <= max(1, 0.1 * ref_it) and res < 1e-8
+    del rows

@@ -122,3 +122,21 @@ def test_grad_logk_matches_finite_differences(bs, kw):
         lm = s.logk.copy(); lm[i] -= h
         fd[i] = W @ (gen.generate_from_logk(p, lp).v - gen.generate_from_logk(p, lm).v) / (2 * h)
     np.testing.assert_allclose(g, fd, rtol=1e-6, atol=1e-8 * np.abs(fd).max())
+
+
+def test_batch_blocks_and_subset():
+    r, c, v, ro, B, shapes = gen.batch(5, seed=3, cells_lo=60, cells_hi=600, nrhs=4)
+    assert len(ro) == 6 and ro[-1] == len(r) - 1 and len(B) == ro[-1] * 4
+    rows = np.repeat(np.arange(ro[-1]), np.diff(r))
+    sys_of = np.searchsorted(ro, rows, side="right") - 1
+    assert (np.searchsorted(ro, c, side="right") - 1 == sys_of).all()  # block-diagonal
+    cells = np.diff(ro) // 2
+    assert (cells >= 2).all()
+    r2, c2, v2, ro2, B2 = gen.batch_subset(r, c, v, ro, B, 4, [1, 3])
+    for k, q in enumerate([1, 3]):
+        a, e = ro[q], ro[q + 1]
+        a2, e2 = ro2[k], ro2[k + 1]
+        np.testing.assert_array_equal(r2[a2:e2 + 1] - r2[a2], r[a:e + 1] - r[a])
+        np.testing.assert_array_equal(c2[r2[a2]:r2[e2]] - a2, c[r[a]:r[e]] - a)
+        np.testing.assert_array_equal(v2[r2[a2]:r2[e2]], v[r[a]:r[e]])
+        np.testing.assert_array_equal(B2.reshape(-1, 4)[a2:e2], B.reshape(-1, 4)[a:e])

@@ -62,20 +62,27 @@ def test_batch_matches_single_solves(d, nrhs, restart):
             assert rel(X[ro[q]:ro[q + 1], k], S1.x.cpu().numpy()) < 1e-6
 
 
-def test_batch_graph_and_direct_launches_agree(d):
+def test_batch_launch_modes_agree(d):
+    """One graph launch with the device-side cycle loop (default), the cycle graph
+    relaunched by the host, and direct launches: bit-identical results; restart 10
+    makes the loop run several cycles."""
     r, c, v, ro, B, _ = gen.batch(4, seed=5, cells_lo=100, cells_hi=800, nrhs=4)
     n = int(ro[-1])
     out = []
-    for graph in ("1", "0"):
-        os.environ["DECO_BATCH_GRAPH"] = graph
+    for mode in ("2", "1", "0"):
+        os.environ["DECO_BATCH_GRAPH"] = mode
         try:
             Bt = d.Batch(cpr_json(2), d.CSR(n, n, r, c, v), ro, 4)
-            out.append((Bt.solve(sol_json(), cuda(B)).cpu().numpy(), Bt.iters.copy(), Bt.result["graph"]))
+            X = Bt.solve(sol_json(restart=10), cuda(B)).cpu().numpy()
+            out.append((X, Bt.iters.copy(), Bt.result["graph"], Bt.result["cycles"]))
+            assert (Bt.flags == 0).all()
         finally:
             os.environ.pop("DECO_BATCH_GRAPH", None)
-    assert out[0][2] and not out[1][2]
-    np.testing.assert_array_equal(out[0][0], out[1][0])
-    np.testing.assert_array_equal(out[0][1], out[1][1])
+    assert [o[2] for o in out] == [2, 1, 0]
+    assert out[0][3] == out[1][3] == out[2][3] > 1
+    for o in out[1:]:
+        np.testing.assert_array_equal(out[0][0], o[0])
+        np.testing.assert_array_equal(out[0][1], o[1])
 
 
 def test_batch_mixed_precision(d):

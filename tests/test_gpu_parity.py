@@ -98,13 +98,15 @@ def test_residual(d, oracle):
 
 @pytest.mark.parametrize("name", ["c1", "bs3_faults"])
 @pytest.mark.parametrize("tols", [(0.0, 0.0), (0.0, 1e-16), (0.2, 1e-16)])
-def test_fsai_matches_reference(d, oracle, name, tols):
+@pytest.mark.parametrize("power", [1, 2])
+def test_fsai_matches_reference(d, oracle, name, tols, power):
+    """power 2: the lower(A A) pattern (symbolic.tpp:149-172), local systems of larger order."""
     _, ref = oracle
     s = system(name)
     A = d.CSR.from_system(s)
-    F = d.FSAI({"tol_rel": tols[0], "tol_abs": tols[1], "power": 1}, A)
+    F = d.FSAI({"tol_rel": tols[0], "tol_abs": tols[1], "power": power}, A)
     (Lr, Lc, Lv), (Ur, Uc, Uv) = F.factors()
-    R = ref.Fsai(s.r, s.c, s.v, tols[0], tols[1], 1)
+    R = ref.Fsai(s.r, s.c, s.v, tols[0], tols[1], power)
     (RLr, RLc, RLv), (RUr, RUc, RUv) = R.factors()
     # pattern: bit-exact
     for a, b in [(Lr, RLr), (Lc, RLc), (Ur, RUr), (Uc, RUc)]:
@@ -133,6 +135,7 @@ CPR_CASES = {
     "qimpes_seq0": dict(weights="quasiimpes", seq=0),
     "seq1_glo_filter": dict(seq=1, glo_rel=0.2),
     "tol_zero": dict(tol_zero=1e-14),
+    "power2": dict(glo_power=2, loc_power=2),
     "no_weights": dict(weights="none"),
 }
 

@@ -62,7 +62,8 @@ LIVE = {
 
 
 @pytest.mark.parametrize("name", list(LIVE))
-@pytest.mark.parametrize("case", [dict(), dict(drs=1, e_ps=0.5), dict(seq=0, glo_rel=0.2)])
+@pytest.mark.parametrize("case", [dict(), dict(drs=1, e_ps=0.5), dict(seq=0, glo_rel=0.2),
+                                  dict(glo_power=2, loc_power=2)])
 def test_port_matches_reference_live(name, case):
     from deco_b200 import gen
     from oracle import port, ref
