@@ -36,7 +36,6 @@ namespace {
 
 constexpr int kT = 256;            // threads per block of the batch kernels
 constexpr int kChunkRows = 4096;   // rows per dot chunk (chunks never cross systems)
-constexpr int kGroup = 16;         // basis columns per block of pass A
 constexpr double kEpsB = 2.220446049250312e-16;
 
 // per-instance state, `stride` doubles each: H (m+1)m | G (m+1)^2 | g | cs | sn | s | c | misc
@@ -175,44 +174,157 @@ __global__ void b_sys_active(int nsys, Inst in) {
   in.sys_active[sys] = a;
 }
 
-// ---- pass A: raw dots u_i . w and u_i . u_j for i in [i0, i0 + kGroup) ∩ [0, j], per (chunk, k)
+// ---- vector access for the dot and update passes: a thread moves Ev consecutive
+// elements of a multi-vector per load (16 bytes when K allows: float4 / double2),
+// all of one row, so they belong to instances Ev*p .. Ev*p + Ev - 1 where the
+// phase p = (element / Ev) % (K / Ev) is fixed for a thread over its whole sweep.
+template <typename T, int E> struct VecN;
+template <> struct VecN<float, 4> { using t = float4; };
+template <> struct VecN<float, 2> { using t = float2; };
+template <> struct VecN<float, 1> { using t = float; };
+template <> struct VecN<double, 2> { using t = double2; };
+template <> struct VecN<double, 1> { using t = double; };
+
+template <typename T, int E>
+__device__ __forceinline__ void vload(const T* __restrict__ p, double* o, bool stream) {
+  using V = typename VecN<T, E>::t;
+  const V v = stream ? __ldcs(reinterpret_cast<const V*>(p)) : __ldg(reinterpret_cast<const V*>(p));
+  if constexpr (E == 1) {
+    o[0] = (double)v;
+  } else {
+    const T* e = reinterpret_cast<const T*>(&v);
+#pragma unroll
+    for (int q = 0; q < E; ++q) o[q] = (double)e[q];
+  }
+}
+template <typename T, int E>
+__device__ __forceinline__ void vstore(T* p, const T* o) {
+  using V = typename VecN<T, E>::t;
+  *reinterpret_cast<V*>(p) = *reinterpret_cast<const V*>(o);
+}
+
+template <int K, typename T> struct VShape {
+  static constexpr int E = (16 / (int)sizeof(T)) < K ? (16 / (int)sizeof(T)) : K;  // elements per load
+  static constexpr int P = K / E;                                                  // phases
+  static constexpr int G = 16 / E;                                                 // columns per dot block
+};
+
+// Sums acc[s] (s < NS slots) over the block's threads of equal phase, in a fixed
+// order; returns in `out` (shared, [P][NS]) the totals per (phase, slot).
+template <int P, int NS>
+__device__ __forceinline__ void reduce_phase(const double* acc, double* part /* [kT/32][P][NS] */, int phase0,
+                                             double* out /* [P][NS] */) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int s2 = 0; s2 < NS; ++s2) {
+    double v = acc[s2];
+#pragma unroll
+    for (int o = 16; o >= P; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane < P) part[(warp * P + (phase0 + lane) % P) * NS + s2] = v;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < P * NS; t += blockDim.x) {
+    double sum = 0.0;
+    for (int w = 0; w < kT / 32; ++w) sum += part[w * P * NS + t];
+    out[t] = sum;
+  }
+  __syncthreads();
+}
+
+// ---- pass A (vectorised): raw dots u_i . w and u_i . u_j for the block's group of
+// G columns, per (chunk, instance)
 template <int K, typename T>
-__global__ void __launch_bounds__(kT) b_dots(const int* crow, const int* csys, Inst in, long long ld, int j,
-                                             const T* __restrict__ V, const T* __restrict__ w, double* __restrict__ red,
-                                             int nchunk) {
-  __shared__ double sm[(kT / 32) * K];
-  const int c = blockIdx.x, i0 = blockIdx.y * kGroup;
-  const int ni = min(kGroup, j + 1 - i0);
-  const int k = threadIdx.x % K;
+__global__ void __launch_bounds__(kT) b_dots_v(const int* crow, const int* csys, Inst in, long long ld, int j,
+                                               const T* __restrict__ V, const T* __restrict__ w,
+                                               double* __restrict__ red, int nchunk) {
+  using S = VShape<K, T>;
+  constexpr int E = S::E, P = S::P, G = S::G, NS = 2 * E * G;
+  __shared__ double part[(kT / 32) * P * NS];
+  __shared__ double tot[P * NS];
+  const int c = blockIdx.x, i0 = blockIdx.y * G;
+  const int ni = min(G, j + 1 - i0);
   const bool live = chunk_live(csys, in.sys_active, c);
-  double ph[kGroup], pg[kGroup];
+  const long long f0 = (long long)crow[c] * K / E, f1 = (long long)crow[c + 1] * K / E;
+  double acc[NS];
 #pragma unroll
-  for (int t = 0; t < kGroup; ++t) { ph[t] = 0.0; pg[t] = 0.0; }
+  for (int t = 0; t < NS; ++t) acc[t] = 0.0;
   if (live) {
-    const long long e0 = (long long)crow[c] * K, e1 = (long long)crow[c + 1] * K;
     const T* __restrict__ uj = V + (long long)j * ld;
-    for (long long e = e0 + threadIdx.x; e < e1; e += kT) {
-      const double we = (double)w[e], ue = (double)uj[e];
+    for (long long f = f0 + threadIdx.x; f < f1; f += kT) {
+      double wv[E], uv[E];
+      vload<T, E>(w + f * E, wv, false);
+      vload<T, E>(uj + f * E, uv, false);
 #pragma unroll
-      for (int t = 0; t < kGroup; ++t)
-        if (t < ni) {
-          const double v = (double)__ldcs(V + (long long)(i0 + t) * ld + e);
-          ph[t] += v * we;
-          pg[t] += v * ue;
+      for (int t = 0; t < G; ++t) {
+        if (t < ni) {  // uniform over the block
+          double v[E];
+          vload<T, E>(V + (long long)(i0 + t) * ld + f * E, v, true);
+#pragma unroll
+          for (int q = 0; q < E; ++q) {
+            acc[t * E + q] += v[q] * wv[q];
+            acc[(G + t) * E + q] += v[q] * uv[q];
+          }
         }
+      }
     }
   }
-  // slots: h at i*K + k, Gram at (m_slots + i)*K + k — red holds 2 * (j+1) * K rows of nchunk
+  reduce_phase<P, NS>(acc, part, (int)(f0 % P), tot);
   const int nc = j + 1;
-#pragma unroll
-  for (int t = 0; t < kGroup; ++t) {
-    if (t >= ni) break;
-    double o;
-    reduce_k<K>(ph[t], sm, &o);
-    if (threadIdx.x < K) red[((long long)(i0 + t) * K + k) * nchunk + c] = live ? o : 0.0;
-    reduce_k<K>(pg[t], sm, &o);
-    if (threadIdx.x < K) red[((long long)(nc + i0 + t) * K + k) * nchunk + c] = live ? o : 0.0;
+  for (int t2 = threadIdx.x; t2 < P * NS; t2 += kT) {
+    const int ph = t2 / NS, sl = t2 % NS;
+    const int gram = sl / (G * E), t = (sl / E) % G, q = sl % E;
+    if (t >= ni) continue;
+    const int k = E * ph + q;
+    const int col = (gram ? nc : 0) + i0 + t;
+    red[((long long)col * K + k) * nchunk + c] = live ? tot[t2] : 0.0;
   }
+}
+
+// ---- pass B (vectorised): u_{j+1} = w - sum_i c_i u_i; partial ||u_{j+1}||^2 per instance
+template <int K, typename T>
+__global__ void __launch_bounds__(kT) b_update_v(const int* crow, const int* csys, BState st, Inst in, long long ld,
+                                                 int j, const T* __restrict__ V, const T* __restrict__ w,
+                                                 T* __restrict__ out, double* __restrict__ red, int nchunk) {
+  using S = VShape<K, T>;
+  constexpr int E = S::E, P = S::P;
+  __shared__ double cf[64][K];
+  __shared__ double part[(kT / 32) * P * E];
+  __shared__ double tot[P * E];
+  const int c = blockIdx.x, sys = csys[c], nc = j + 1;
+  if (!in.sys_active[sys]) {
+    if (threadIdx.x < K) red[(long long)threadIdx.x * nchunk + c] = 0.0;
+    return;
+  }
+  for (int t = threadIdx.x; t < K * nc; t += kT) {
+    const int i = t / K, kk = t % K, qi = sys * K + kk;
+    cf[i][kk] = in.active[qi] ? st.c(qi)[i] : 0.0;
+  }
+  __syncthreads();
+  const long long f0 = (long long)crow[c] * K / E, f1 = (long long)crow[c + 1] * K / E;
+  const int ph = (int)((f0 + threadIdx.x) % P);
+  double ss[E];
+#pragma unroll
+  for (int q = 0; q < E; ++q) ss[q] = 0.0;
+  for (long long f = f0 + threadIdx.x; f < f1; f += kT) {
+    double x[E];
+    vload<T, E>(w + f * E, x, false);
+#pragma unroll 4
+    for (int i = 0; i < nc; ++i) {
+      double v[E];
+      vload<T, E>(V + (long long)i * ld + f * E, v, true);
+#pragma unroll
+      for (int q = 0; q < E; ++q) x[q] -= cf[i][E * ph + q] * v[q];
+    }
+    T o[E];
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+      o[q] = (T)x[q];
+      ss[q] += (double)o[q] * (double)o[q];
+    }
+    vstore<T, E>(out + f * E, o);
+  }
+  reduce_phase<P, E>(ss, part, (int)(f0 % P), tot);
+  for (int t2 = threadIdx.x; t2 < P * E; t2 += kT) red[(long long)t2 * nchunk + c] = tot[t2];
 }
 
 // one warp per instance: h, the Gram row of u_j, c = h + (h - G h), H(:,j), coefficients
@@ -245,38 +357,6 @@ __global__ void b_dots_fin(int Q, const int* sch, BState st, Inst in, int j, con
     st.H(qi, i, j) = ci;
     st.c(qi)[i] = ci * s[i];
   }
-}
-
-// ---- pass B: u_{j+1} = w - sum_i c_i u_i (per instance coefficients); partial ||u_{j+1}||^2
-template <int K, typename T>
-__global__ void __launch_bounds__(kT) b_update(const int* crow, const int* csys, BState st, Inst in, long long ld,
-                                               int j, const T* __restrict__ V, const T* __restrict__ w,
-                                               T* __restrict__ out, double* __restrict__ red, int nchunk) {
-  __shared__ double sm[(kT / 32) * K];
-  __shared__ double cf[K][64];
-  const int c = blockIdx.x, sys = csys[c], nc = j + 1;
-  const int k = threadIdx.x % K;
-  if (!in.sys_active[sys]) {
-    if (threadIdx.x < K) red[(long long)threadIdx.x * nchunk + c] = 0.0;
-    return;
-  }
-  for (int t = threadIdx.x; t < K * nc; t += kT) {
-    const int kk = t / nc, i = t % nc, qi = sys * K + kk;
-    cf[kk][i] = in.active[qi] ? st.c(qi)[i] : 0.0;
-  }
-  __syncthreads();
-  const long long e0 = (long long)crow[c] * K, e1 = (long long)crow[c + 1] * K;
-  double ss = 0.0;
-  for (long long e = e0 + threadIdx.x; e < e1; e += kT) {
-    double x = (double)w[e];
-    for (int i = 0; i < nc; ++i) x -= cf[k][i] * (double)__ldcs(V + (long long)i * ld + e);
-    const T o = (T)x;
-    out[e] = o;
-    ss += (double)o * (double)o;
-  }
-  double o;
-  reduce_k<K>(ss, sm, &o);
-  if (threadIdx.x < K) red[(long long)k * nchunk + c] = o;
 }
 
 __device__ void b_givens_make(double x, double y, double& c, double& s) {
@@ -619,12 +699,13 @@ struct BatchSolver {
       else
         spmm<K, double, T>(ctx, B->A, z.get(), MStoreScaled<K, T>{w.get(), st.base + soff + j, st.stride,
                                                                    B->cell_sys.get(), B->bs}, false, inner_gate());
-      const int ngroups = (j + 1 + kGroup - 1) / kGroup;
-      b_dots<K, T><<<dim3(nch, ngroups), kT, 0, s>>>(crow, csys, in, ld, j, V.get(), w.get(), red.get(), nch);
+      constexpr int G = VShape<K, T>::G;
+      const int ngroups = (j + 1 + G - 1) / G;
+      b_dots_v<K, T><<<dim3(nch, ngroups), kT, 0, s>>>(crow, csys, in, ld, j, V.get(), w.get(), red.get(), nch);
       DECO_CHECK_LAUNCH();
       b_dots_fin<K><<<(int)cdiv(Q, kT / 32), kT, 0, s>>>(Q, sch, st, in, j, red.get(), nch);
       DECO_CHECK_LAUNCH();
-      b_update<K, T><<<nch, kT, 0, s>>>(crow, csys, st, in, ld, j, V.get(), w.get(), col(j + 1), red.get(), nch);
+      b_update_v<K, T><<<nch, kT, 0, s>>>(crow, csys, st, in, ld, j, V.get(), w.get(), col(j + 1), red.get(), nch);
       DECO_CHECK_LAUNCH();
       b_update_fin<K><<<qb, 128, 0, s>>>(Q, sch, st, in, j, red.get(), nch, prm.reltol, prm.itmax);
       DECO_CHECK_LAUNCH();
