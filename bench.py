@@ -532,8 +532,13 @@ def main():
         k["frac_of_peak"] = k["gbs"] / peak
     dom = kernels["spmv_A_f32"]
     roofline = {"bound": "hbm", "achieved": dom["gbs"], "peak": peak, "unit": "GB/s", "frac": dom["gbs"] / peak,
-                "traffic": None,
-                "kernel": ("deco::bsr_kernel<float> (cell blocks)" if A.blocks[0] else "deco::spmv_kernel<float> (CSR)")
+                # DRAM read + write bytes per launch of this kernel from one ncu capture of this
+                # workload (profiles/bsr2_pair_f32_config3_full.md): 633.9 MB read + 10.6 MB written
+                "traffic": 644.5e6 if A.blocks[0] == 2 else None,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/bsr2_pair_f32_config3_full.md"
+                if A.blocks[0] == 2 else None,
+                "kernel": {2: "deco::bsr2_pair_kernel<float> (2x2 cell blocks)",
+                           3: "deco::bsr_kernel<float> (3x3 cell blocks)"}.get(A.blocks[0], "deco::spmv_kernel<float> (CSR)")
                 + " on A (8M rows, 111.36M nnz, float32 values)",
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind}
 

@@ -37,8 +37,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kColsPerWarp = 8;
-constexpr int kMaxCols = kWarps * kColsPerWarp;  // basis columns pass A handles (restart <= 63)
+constexpr int kMaxCols = kWarps * 8;  // basis columns pass A handles, 8 per warp (restart <= 63)
 // host read-back of |g_{j+1}|: a ring of kRing pinned slots (from kSlot0) and
 // events; the host runs up to `lookahead` Arnoldi steps ahead (<= kRing - 2)
 constexpr int kRing = 8;
@@ -174,19 +173,139 @@ __device__ void dots_finish(int ncols, int j, const double* __restrict__ red, St
 }
 
 
+// 16-byte copy global -> shared that does not pass through registers (cp.async,
+// completion tracked per thread by commit / wait groups)
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// partial dot of one float4 pair, returned in float64: the four products are
+// summed in float32 (about one rounding per product, the size of the rounding the
+// stored basis itself carries) and converted once, so a float32 element costs a
+// quarter of a conversion instead of two
+__device__ __forceinline__ double vdot(const float4& a, const float4& b) {
+  return (double)fmaf(a.w, b.w, fmaf(a.z, b.z, fmaf(a.y, b.y, a.x * b.x)));
+}
+
 // ---- pass A: raw dots u_c . w and u_c . u_j for c < ncols (u = stored columns).
-// Blocks own contiguous ranges of 128-bit vectors; warp w owns columns w, w+8, ...;
-// lanes keep per-column partial sums in registers for the whole range (no
-// barriers; w and u_j are shared through L1 by the block's warps).  Rows past the
-// last full vector are summed by the last block.  (Measured on B200 for the
-// float32 basis at restart 50 on the 8M-row system: sweeping column groups with
-// block reductions took 0.51 ms per iteration for the whole orthogonalisation
-// against 0.44 ms here; staging the tiles through shared memory with a
-// three-deep cp.async pipeline, 0.45 ms.)
-template <typename T>
+// Blocks own contiguous ranges of 128-bit vectors, walked in tiles of kTileVec;
+// the tiles of w and u_j are copied into shared memory (double-buffered cp.async,
+// so the next tile streams in while this one is used) and warp w streams columns
+// w, w+8, ... (CPW of them: the template is the smallest power of two with
+// 8*CPW >= ncols) against them, keeping per-column partial sums in registers.
+// Rows past the last full vector are summed by the last block.  (Measured on
+// B200, float32 basis, 8M rows, 26 columns: 168 us against 370 us when every
+// warp held w and u_j in registers and formed each product in float64; the
+// float32 conversions, not the loads, bounded that form.)
+constexpr int kTileVec = 512;
+constexpr int kVecPerLane = 4;
+template <typename T, int CPW>  // T = float
 __global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long ld, int ncols, int j,
                                                          const T* __restrict__ V, const T* __restrict__ w,
                                                          double* __restrict__ red, unsigned* counter, State st) {
+  using VT = typename Vec4<T>::t;
+  constexpr int N = Vec4<T>::N;
+  static_assert(kTileVec % (32 * kVecPerLane) == 0, "tile must hold whole lane steps");
+  __shared__ __align__(16) VT ws[2][kTileVec];
+  __shared__ __align__(16) VT us[2][kTileVec];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long nvec = n / N;
+  const long long per = (nvec + gridDim.x - 1) / gridDim.x;
+  const long long v0 = min(nvec, per * blockIdx.x), v1 = min(nvec, v0 + per);
+  const VT* __restrict__ wv4 = reinterpret_cast<const VT*>(w);
+  const VT* __restrict__ uv4 = reinterpret_cast<const VT*>(V + (size_t)j * ld);
+  double pw[CPW], pu[CPW];
+#pragma unroll
+  for (int k = 0; k < CPW; ++k) { pw[k] = 0.0; pu[k] = 0.0; }
+  const int ntiles = (int)((v1 - v0 + kTileVec - 1) / kTileVec);
+  auto load_tile = [&](int t, int buf) {
+    const long long t0 = v0 + (long long)t * kTileVec;
+    for (int i = threadIdx.x; i < kTileVec; i += kThreads) {
+      const long long vi = t0 + i;
+      if (vi < v1) {
+        cp_async16(&ws[buf][i], wv4 + vi);
+        cp_async16(&us[buf][i], uv4 + vi);
+      } else {
+        ws[buf][i] = Vec4<T>::zero();
+        us[buf][i] = Vec4<T>::zero();
+      }
+    }
+    cp_async_commit();
+  };
+  if (ntiles > 0) load_tile(0, 0);
+  for (int t = 0; t < ntiles; ++t) {
+    const int buf = t & 1;
+    if (t + 1 < ntiles) {
+      load_tile(t + 1, buf ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const long long t0 = v0 + (long long)t * kTileVec;
+#pragma unroll
+    for (int k = 0; k < CPW; ++k) {
+      const int c = warp + k * kWarps;
+      if (c < ncols) {
+        const VT* __restrict__ vc = reinterpret_cast<const VT*>(V + (size_t)c * ld);
+        for (int s0 = 0; s0 < kTileVec; s0 += 32 * kVecPerLane) {
+          VT v[kVecPerLane];
+#pragma unroll
+          for (int q = 0; q < kVecPerLane; ++q) {
+            const long long vi = t0 + s0 + lane + 32 * q;
+            v[q] = vi < v1 ? __ldcs(vc + vi) : Vec4<T>::zero();
+          }
+#pragma unroll
+          for (int q = 0; q < kVecPerLane; ++q) {
+            const int si = s0 + lane + 32 * q;
+            pw[k] += vdot(v[q], ws[buf][si]);
+            pu[k] += vdot(v[q], us[buf][si]);
+          }
+        }
+      }
+    }
+    __syncthreads();  // buffer `buf` is refilled by the next iteration's copy
+  }
+  if (blockIdx.x == gridDim.x - 1 && lane == 0) {  // rows past the last full vector
+    const T* __restrict__ uj = V + (size_t)j * ld;
+    for (long long r = nvec * N; r < n; ++r)
+#pragma unroll
+      for (int k = 0; k < CPW; ++k) {
+        const int c = warp + k * kWarps;
+        if (c < ncols) {
+          const double v = (double)V[(size_t)c * ld + r];
+          pw[k] += v * (double)w[r];
+          pu[k] += v * (double)uj[r];
+        }
+      }
+  }
+#pragma unroll
+  for (int k = 0; k < CPW; ++k) {
+    const int c = warp + k * kWarps;
+    const double a = warp_sum(pw[k]), b = warp_sum(pu[k]);
+    if (lane == 0 && c < ncols) {
+      red[(size_t)c * gridDim.x + blockIdx.x] = a;
+      red[(size_t)(ncols + c) * gridDim.x + blockIdx.x] = b;
+    }
+  }
+  if (!last_block(counter)) return;
+  dots_finish(ncols, j, red, st);
+}
+
+// ---- pass A for the float64 basis: the same dots with w and u_j held in
+// registers: warp w owns columns w, w+8, ...; each lane loads its 128-bit vectors
+// of w and u_j once per step and streams its columns against them (no barriers;
+// the block's warps share w and u_j through L1).  Measured on B200 at restart 50
+// on the 8M-row system: 0.62 ms per iteration for the whole orthogonalisation,
+// against 0.83 ms with the shared-memory tiles of the float32 form.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) arnoldi_dots_reg(long long n, long long ld, int ncols, int j,
+                                                             const T* __restrict__ V, const T* __restrict__ w,
+                                                             double* __restrict__ red, unsigned* counter, State st) {
   using VT = typename Vec4<T>::t;
   constexpr int N = Vec4<T>::N;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -195,10 +314,9 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long 
   const long long v0 = per * blockIdx.x, v1 = min(nvec, v0 + per);
   const VT* __restrict__ wv4 = reinterpret_cast<const VT*>(w);
   const VT* __restrict__ uv4 = reinterpret_cast<const VT*>(V + (size_t)j * ld);
-  double pw[kColsPerWarp], pu[kColsPerWarp];
+  double pw[8], pu[8];
 #pragma unroll
-  for (int k = 0; k < kColsPerWarp; ++k) { pw[k] = 0.0; pu[k] = 0.0; }
-  constexpr int kVecPerLane = 4;
+  for (int k = 0; k < 8; ++k) { pw[k] = 0.0; pu[k] = 0.0; }
   for (long long base = v0; base < v1; base += 32 * kVecPerLane) {
     VT wv[kVecPerLane], uv[kVecPerLane];
 #pragma unroll
@@ -208,7 +326,7 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long 
       uv[q] = vi < v1 ? uv4[vi] : Vec4<T>::zero();
     }
 #pragma unroll
-    for (int k = 0; k < kColsPerWarp; ++k) {
+    for (int k = 0; k < 8; ++k) {
       const int c = warp + k * kWarps;
       if (c < ncols) {
         const VT* __restrict__ vc = reinterpret_cast<const VT*>(V + (size_t)c * ld);
@@ -230,7 +348,7 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long 
     const T* __restrict__ uj = V + (size_t)j * ld;
     for (long long r = nvec * N; r < n; ++r)
 #pragma unroll
-      for (int k = 0; k < kColsPerWarp; ++k) {
+      for (int k = 0; k < 8; ++k) {
         const int c = warp + k * kWarps;
         if (c < ncols) {
           const double v = (double)V[(size_t)c * ld + r];
@@ -240,7 +358,7 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long 
       }
   }
 #pragma unroll
-  for (int k = 0; k < kColsPerWarp; ++k) {
+  for (int k = 0; k < 8; ++k) {
     const int c = warp + k * kWarps;
     const double a = warp_sum(pw[k]), b = warp_sum(pu[k]);
     if (lane == 0 && c < ncols) {
@@ -250,6 +368,21 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long 
   }
   if (!last_block(counter)) return;
   dots_finish(ncols, j, red, st);
+}
+
+template <typename T>
+void launch_arnoldi_dots(cudaStream_t s, int nb, long long n, long long ld, int nc, int j, const T* V, const T* w,
+                         double* red, unsigned* counter, State st) {
+  if constexpr (std::is_same<T, double>::value)
+    arnoldi_dots_reg<T><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V, w, red, counter, st);
+  else if (nc <= kWarps)
+    arnoldi_dots<T, 1><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V, w, red, counter, st);
+  else if (nc <= 2 * kWarps)
+    arnoldi_dots<T, 2><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V, w, red, counter, st);
+  else if (nc <= 4 * kWarps)
+    arnoldi_dots<T, 4><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V, w, red, counter, st);
+  else
+    arnoldi_dots<T, 8><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V, w, red, counter, st);
 }
 
 // ---- pass B: w'' = w - sum_c coef_c u_c, stored as column j+1; ||w''||^2.
@@ -521,7 +654,7 @@ struct Solver {
     }
     if (profile) DECO_CUDA(cudaEventRecord(pev[4 * j + 2], s));
     const int nc = j + 1;
-    arnoldi_dots<T><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V.get(), w.get(), ctx->red.get(), ctx->counter.get(), st);
+    launch_arnoldi_dots<T>(s, nb, n, ld, nc, j, V.get(), w.get(), ctx->red.get(), ctx->counter.get(), st);
     DECO_CHECK_LAUNCH();
     arnoldi_update<T><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V.get(), w.get(), col(j + 1), ctx->red.get(),
                                               ctx->counter.get(), st);
