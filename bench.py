@@ -523,18 +523,26 @@ def main():
     P32 = d.CPR(PREC, d.CSR(n, n, r_d, c_d, v_d, ctx), b_d.clone(), precision=32)
     Fg32 = P32.fsai(0)
     fb, kl, ku = Fg32.blocks
-    ms = kernel_ms(lambda: Fg32.apply(x64, y64))
-    algF32 = matrix_bytes(nzF, (fb, kl), 4) + matrix_bytes(nzF, (fb, ku), 4) + 8 * n + 2 * 4 * n + 8 * n
+    # as the mixed-precision CPR applies it: float32 x, intermediate and y
+    ms = kernel_ms(lambda: Fg32.apply_f32(x32, y32))
+    algF32 = matrix_bytes(nzF, (fb, kl), 4) + matrix_bytes(nzF, (fb, ku), 4) + 4 * n + 2 * 4 * n + 4 * n
     kernels["fsai_apply_global_f32"] = {"ms": ms, "gbs": algF32 / ms / 1e6, "alg_bytes": algF32,
-                                        "format": "cell-block (bs %d)" % fb if fb else "CSR"}
+                                        "format": "cell-block (bs %d)" % fb if fb else "CSR",
+                                        "vectors": "float32 (deco_fsai_apply_f32)"}
+    # through the reference-shaped interface: float64 x and y around the float32 factor
+    ms = kernel_ms(lambda: Fg32.apply(x64, y64))
+    algF32d = matrix_bytes(nzF, (fb, kl), 4) + matrix_bytes(nzF, (fb, ku), 4) + 8 * n + 2 * 4 * n + 8 * n
+    kernels["fsai_apply_global_f32_f64io"] = {"ms": ms, "gbs": algF32d / ms / 1e6, "alg_bytes": algF32d,
+                                              "format": "cell-block (bs %d)" % fb if fb else "CSR",
+                                              "vectors": "float64 (deco_fsai_apply)"}
     del P32
     for k in kernels.values():
         k["frac_of_peak"] = k["gbs"] / peak
     dom = kernels["spmv_A_f32"]
     roofline = {"bound": "hbm", "achieved": dom["gbs"], "peak": peak, "unit": "GB/s", "frac": dom["gbs"] / peak,
                 # DRAM read + write bytes per launch of this kernel from one ncu capture of this
-                # workload (profiles/bsr2_pair_f32_config3_full.md): 633.9 MB read + 10.6 MB written
-                "traffic": 644.5e6 if A.blocks[0] == 2 else None,
+                # workload (profiles/bsr2_pair_f32_config3_full.md): 604.8 MB read + 11.5 MB written
+                "traffic": 616.3e6 if A.blocks[0] == 2 else None,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/bsr2_pair_f32_config3_full.md"
                 if A.blocks[0] == 2 else None,
                 "kernel": {2: "deco::bsr2_pair_kernel<float> (2x2 cell blocks)",

@@ -257,6 +257,15 @@ class FSAI:
         check(lib().deco_fsai_apply(self.ctx.h, self.h, _ptr(x), _ptr(b)))
         return b
 
+    def apply_f32(self, x, b=None):
+        """b = FU^T (FL x) in float32 vectors (a factor made with precision 32)."""
+        torch = _torch()
+        x = _dev(x, torch.float32)
+        if b is None:
+            b = torch.empty(self.n, dtype=torch.float32, device="cuda")
+        check(lib().deco_fsai_apply_f32(self.ctx.h, self.h, _ptr(x), _ptr(b)))
+        return b
+
     @property
     def blocks(self):
         """(block size, stored blocks of FL, stored blocks of FU^T); block size 0 without block copies."""

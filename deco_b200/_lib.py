@@ -72,6 +72,7 @@ SIGNATURES = {
     "deco_fsai_blocks": ([vp, ip, ip, ip], C.c_int),
     "deco_fsai_download": ([vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
     "deco_fsai_apply": ([vp, vp, vp, vp], C.c_int),
+    "deco_fsai_apply_f32": ([vp, vp, vp, vp], C.c_int),
     "deco_fsai_apply_static": ([vp, vp, vp, vp], C.c_int),
     "deco_cpr_create": ([vp, vp, vp, C.POINTER(CprParams), C.POINTER(vp)], C.c_int),
     "deco_cpr_destroy": ([vp], C.c_int),

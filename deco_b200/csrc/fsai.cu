@@ -783,4 +783,12 @@ int deco_fsai_apply(deco_ctx ctx, deco_fsai F, const double* x, double* y) {
   });
 }
 
+int deco_fsai_apply_f32(deco_ctx ctx, deco_fsai F, const float* x, float* y) {
+  return guard([&] {
+    DECO_REQUIRE(ctx && F && x && y, DECO_ERR_ARG, "NULL argument");
+    DECO_REQUIRE(F->precision == 32, DECO_ERR_ARG, "deco_fsai_apply_f32 needs a factor made with precision 32");
+    fsai_apply_t<float, float, float>(ctx, F, x, F->tmp32.get(), EpiStore<float>{y});
+  });
+}
+
 }  // extern "C"

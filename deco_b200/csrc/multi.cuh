@@ -78,6 +78,21 @@ __device__ __forceinline__ void load_k(const XT* __restrict__ x, long long o, do
   }
 }
 
+// K consecutive float32 values from x + o (o a multiple of K), as float32
+template <int K>
+__device__ __forceinline__ void load_k_f32(const float* __restrict__ x, long long o, float* out) {
+  if constexpr (K % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < K / 4; ++q) {
+      const float4 t = __ldg(reinterpret_cast<const float4*>(x + o) + q);
+      out[4 * q] = t.x; out[4 * q + 1] = t.y; out[4 * q + 2] = t.z; out[4 * q + 3] = t.w;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < K; ++q) out[q] = __ldg(x + o + q);
+  }
+}
+
 // Optional skip of finished systems: block row s is left out (its outputs are
 // not written) when active[cell_sys[s / div]] == 0.
 struct MMGate {
@@ -106,15 +121,36 @@ __global__ void __launch_bounds__(256) bsr_mm_kernel(int nbr, const int* __restr
     const int a = __ldg(br + s), e = __ldg(br + s + 1);
     for (int blk = a + lane; blk < e; blk += SW) {
       const long long col0 = (long long)__ldcs(bc + blk) * BS;
+      if constexpr (BS > 1 && kRunF32<VT, XT>) {
+        // float32 runs over the BS entries of each block row (as the
+        // single-vector cell-block product), accumulated in float64
+        float xv[BS][K];
 #pragma unroll
-      for (int t = 0; t < BS; ++t) {
-        double xv[K];
-        load_k<K, XT>(x, (col0 + t) * K, xv);
+        for (int t = 0; t < BS; ++t) load_k_f32<K>(x, (col0 + t) * K, xv[t]);
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
-          const double w = (double)__ldcs(bv + q * plane + (long long)blk * BS + t);
+          float w[BS];
 #pragma unroll
-          for (int k = 0; k < K; ++k) acc[q][k] += w * xv[k];
+          for (int t = 0; t < BS; ++t) w[t] = __ldcs(bv + q * plane + (long long)blk * BS + t);
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            float run = w[0] * xv[0][k];
+#pragma unroll
+            for (int t = 1; t < BS; ++t) run = fmaf(w[t], xv[t][k], run);
+            acc[q][k] += (double)run;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int t = 0; t < BS; ++t) {
+          double xv[K];
+          load_k<K, XT>(x, (col0 + t) * K, xv);
+#pragma unroll
+          for (int q = 0; q < NR; ++q) {
+            const double w = (double)__ldcs(bv + q * plane + (long long)blk * BS + t);
+#pragma unroll
+            for (int k = 0; k < K; ++k) acc[q][k] += w * xv[k];
+          }
         }
       }
     }

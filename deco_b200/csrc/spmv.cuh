@@ -11,12 +11,15 @@
 //     sub-warps of a warp;
 //   * values and columns stream through with evict-first loads, x is read
 //     through the read-only path (L1/L2 keep the 7-point stencil's x tiles);
-//   * sums accumulate in float64 and are reduced with warp shuffles;
+//   * sums accumulate in float64 (float32 values times float32 x: short runs
+//     of products summed in float32 first) and are reduced with warp shuffles;
 //   * the epilogue fuses the vector operation that follows the product in the
 //     CPR and GMRES sequences (store, accumulate, residual, pressure
 //     restriction, pressure prolongation), so those never cost a pass of
 //     their own.
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
 
 struct deco_csr_s {
@@ -60,6 +63,17 @@ __device__ __forceinline__ int elem(const int2& v, int q) { return q == 0 ? v.x 
 __device__ __forceinline__ int elem(const int4& v, int q) {
   return q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w));
 }
+
+// Float32 values times float32 x: the products of one short run (the entries of
+// one 128-bit value load in CSR, one row of one cell block) are summed in float32
+// and converted once; the runs accumulate in float64.  On B200 a float32 ->
+// float64 conversion issues at about 16 per clock per SM, a quarter of the float64
+// FMA rate, and widening every operand (six conversions per 2x2 block) bounded the
+// float32 product below the HBM roofline: 145 us against 135 us for the 8M-row
+// 2x2-block matrix (67 % against 71 % of the copy bandwidth).  Summing whole rows
+// in float32 (129 us) moved the mixed-precision iteration counts.
+template <typename VT, typename XT>
+constexpr bool kRunF32 = std::is_same<VT, float>::value && std::is_same<XT, float>::value;
 
 // ----------------------------------------------------------------- epilogues
 template <typename YT> struct EpiStore {
@@ -109,10 +123,21 @@ __global__ void __launch_bounds__(256) spmv_kernel(int nrows_out, int row_stride
     for (int k = (a & ~(W - 1)) + lane * W; k < e; k += SW * W) {
       const VV v4 = ld_stream(reinterpret_cast<const VV*>(vv + k));
       const VI c4 = ld_stream(reinterpret_cast<const VI*>(ci + k));
+      const VT* vs = reinterpret_cast<const VT*>(&v4);
+      if constexpr (kRunF32<VT, XT>) {
+        float run = 0.f;
 #pragma unroll
-      for (int q = 0; q < W; ++q) {
-        const int idx = k + q;
-        if (idx >= a && idx < e) sum += elem(v4, q) * (double)__ldg(x + elem(c4, q));
+        for (int q = 0; q < W; ++q) {
+          const int idx = k + q;
+          if (idx >= a && idx < e) run = fmaf(vs[q], __ldg(x + elem(c4, q)), run);
+        }
+        sum += (double)run;
+      } else {
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+          const int idx = k + q;
+          if (idx >= a && idx < e) sum += (double)vs[q] * (double)__ldg(x + elem(c4, q));
+        }
       }
     }
   }
@@ -160,29 +185,40 @@ __global__ void __launch_bounds__(256) bsr_kernel(int nbr, const int* __restrict
   double sum[NR];
 #pragma unroll
   for (int q = 0; q < NR; ++q) sum[q] = 0.0;
+  using XA = typename std::conditional<kRunF32<VT, XT>, float, double>::type;  // x and run type
   if (valid) {
     const int a = __ldg(br + s), e = __ldg(br + s + 1);
     for (int k = a + lane; k < e; k += SW) {
       const long long j = (long long)__ldcs(bc + k) * BS;
-      double xv[BS];
+      XA xv[BS];
       if constexpr (BS == 2) {
         const typename Pair<XT>::V p = __ldg(reinterpret_cast<const typename Pair<XT>::V*>(x + j));
-        xv[0] = (double)p.x;
-        xv[1] = (double)p.y;
+        xv[0] = (XA)p.x;
+        xv[1] = (XA)p.y;
       } else {
 #pragma unroll
-        for (int t = 0; t < BS; ++t) xv[t] = (double)__ldg(x + j + t);
+        for (int t = 0; t < BS; ++t) xv[t] = (XA)__ldg(x + j + t);
       }
 #pragma unroll
       for (int q = 0; q < NR; ++q) {
         const VT* vp = bv + q * plane + (long long)k * BS;
+        XA wv[BS];
         if constexpr (BS == 2) {
           const typename Pair<VT>::V w = __ldcs(reinterpret_cast<const typename Pair<VT>::V*>(vp));
-          sum[q] += (double)w.x * xv[0];
-          sum[q] += (double)w.y * xv[1];
+          wv[0] = (XA)w.x;
+          wv[1] = (XA)w.y;
         } else {
 #pragma unroll
-          for (int t = 0; t < BS; ++t) sum[q] += (double)__ldcs(vp + t) * xv[t];
+          for (int t = 0; t < BS; ++t) wv[t] = (XA)__ldcs(vp + t);
+        }
+        if constexpr (kRunF32<VT, XT>) {
+          float run = wv[0] * xv[0];
+#pragma unroll
+          for (int t = 1; t < BS; ++t) run = fmaf(wv[t], xv[t], run);
+          sum[q] += (double)run;
+        } else {
+#pragma unroll
+          for (int t = 0; t < BS; ++t) sum[q] += wv[t] * xv[t];
         }
       }
     }
@@ -206,21 +242,73 @@ __global__ void __launch_bounds__(256) bsr_kernel(int nbr, const int* __restrict
 // and one 16-byte (float) or two 16-byte (double) loads of their values per
 // plane; blocks outside the row are masked (their loads stay inside the padded
 // arrays: the planes are 16-byte aligned and the index array has slack).
-template <typename T> struct Quad;
-template <> struct Quad<float> {
-  __device__ static void load(const float* p, double* o) {
-    const float4 t = __ldcs(reinterpret_cast<const float4*>(p));
-    o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
+// One pair of blocks as loaded: their two columns and the values of both planes.
+template <typename VT> struct PairLoad;
+template <> struct PairLoad<float> {
+  int2 c;
+  float4 w0, w1;
+  template <bool ROW0>
+  __device__ void load(const int* bc, const float* bv, long long plane, int k) {
+    c = __ldcs(reinterpret_cast<const int2*>(bc + k));
+    w0 = __ldcs(reinterpret_cast<const float4*>(bv + 2LL * k));
+    if (!ROW0) w1 = __ldcs(reinterpret_cast<const float4*>(bv + plane + 2LL * k));
   }
 };
-template <> struct Quad<double> {
-  __device__ static void load(const double* p, double* o) {
-    const double2 t = __ldcs(reinterpret_cast<const double2*>(p));
-    const double2 u = __ldcs(reinterpret_cast<const double2*>(p) + 1);
-    o[0] = t.x; o[1] = t.y; o[2] = u.x; o[3] = u.y;
+template <> struct PairLoad<double> {
+  int2 c;
+  double2 w0a, w0b, w1a, w1b;
+  template <bool ROW0>
+  __device__ void load(const int* bc, const double* bv, long long plane, int k) {
+    c = __ldcs(reinterpret_cast<const int2*>(bc + k));
+    w0a = __ldcs(reinterpret_cast<const double2*>(bv + 2LL * k));
+    w0b = __ldcs(reinterpret_cast<const double2*>(bv + 2LL * k) + 1);
+    if (!ROW0) {
+      w1a = __ldcs(reinterpret_cast<const double2*>(bv + plane + 2LL * k));
+      w1b = __ldcs(reinterpret_cast<const double2*>(bv + plane + 2LL * k) + 1);
+    }
   }
 };
 
+// Adds block h (0 or 1) of a loaded pair times x to the two row sums.
+template <bool ROW0, typename VT, typename XT>
+__device__ __forceinline__ void pair_accumulate(const PairLoad<VT>& L, int h, const XT* __restrict__ x, double& s0,
+                                                double& s1) {
+  const int col = h == 0 ? L.c.x : L.c.y;
+  const typename Pair<XT>::V p = __ldg(reinterpret_cast<const typename Pair<XT>::V*>(x + 2LL * col));
+  if constexpr (kRunF32<VT, XT>) {
+    const float a0 = h == 0 ? L.w0.x : L.w0.z, a1 = h == 0 ? L.w0.y : L.w0.w;
+    s0 += (double)fmaf(a1, p.y, a0 * p.x);
+    if (!ROW0) {
+      const float b0 = h == 0 ? L.w1.x : L.w1.z, b1 = h == 0 ? L.w1.y : L.w1.w;
+      s1 += (double)fmaf(b1, p.y, b0 * p.x);
+    }
+  } else if constexpr (std::is_same<VT, float>::value) {
+    const float a0 = h == 0 ? L.w0.x : L.w0.z, a1 = h == 0 ? L.w0.y : L.w0.w;
+    s0 += (double)a0 * (double)p.x;
+    s0 += (double)a1 * (double)p.y;
+    if (!ROW0) {
+      const float b0 = h == 0 ? L.w1.x : L.w1.z, b1 = h == 0 ? L.w1.y : L.w1.w;
+      s1 += (double)b0 * (double)p.x;
+      s1 += (double)b1 * (double)p.y;
+    }
+  } else {
+    const double2 a = h == 0 ? L.w0a : L.w0b;
+    s0 += a.x * (double)p.x;
+    s0 += a.y * (double)p.y;
+    if (!ROW0) {
+      const double2 b = h == 0 ? L.w1a : L.w1b;
+      s1 += b.x * (double)p.x;
+      s1 += b.y * (double)p.y;
+    }
+  }
+}
+
+// Each lane handles two pairs per loop step (k and k + 2 SW): both pairs' index
+// and value loads are issued before either pair's x gathers, so a lane keeps
+// twice the bytes in flight through the index -> x dependence.  The sums run in
+// the same order as a one-pair-per-step loop.  (Measured on B200, float32 values,
+// L2 flushed: 8M-row system matrix 135 -> 127 us, its lower FSAI factor with four
+// blocks per cell 90 -> 86 us.)
 template <int SW, bool ROW0, typename VT, typename XT, class Epi>
 __global__ void __launch_bounds__(256) bsr2_pair_kernel(int nbr, const int* __restrict__ br, const int* __restrict__ bc,
                                                         const VT* __restrict__ bv, long long plane,
@@ -232,22 +320,16 @@ __global__ void __launch_bounds__(256) bsr2_pair_kernel(int nbr, const int* __re
   double s0 = 0.0, s1 = 0.0;
   if (valid) {
     const int a = __ldg(br + s), e = __ldg(br + s + 1);
-    for (int k = (a & ~1) + 2 * lane; k < e; k += 2 * SW) {
-      const int2 c2 = __ldcs(reinterpret_cast<const int2*>(bc + k));
-      double w0[4], w1[4];
-      Quad<VT>::load(bv + 2LL * k, w0);
-      if (!ROW0) Quad<VT>::load(bv + plane + 2LL * k, w1);
-      if (k >= a) {
-        const typename Pair<XT>::V p = __ldg(reinterpret_cast<const typename Pair<XT>::V*>(x + 2LL * c2.x));
-        s0 += w0[0] * (double)p.x;
-        s0 += w0[1] * (double)p.y;
-        if (!ROW0) { s1 += w1[0] * (double)p.x; s1 += w1[1] * (double)p.y; }
-      }
-      if (k + 1 < e) {
-        const typename Pair<XT>::V p = __ldg(reinterpret_cast<const typename Pair<XT>::V*>(x + 2LL * c2.y));
-        s0 += w0[2] * (double)p.x;
-        s0 += w0[3] * (double)p.y;
-        if (!ROW0) { s1 += w1[2] * (double)p.x; s1 += w1[3] * (double)p.y; }
+    for (int k = (a & ~1) + 2 * lane; k < e; k += 4 * SW) {
+      const int kb = k + 2 * SW;
+      PairLoad<VT> P, Q;
+      P.template load<ROW0>(bc, bv, plane, k);
+      if (kb < e) Q.template load<ROW0>(bc, bv, plane, kb);
+      if (k >= a) pair_accumulate<ROW0, VT, XT>(P, 0, x, s0, s1);
+      if (k + 1 < e) pair_accumulate<ROW0, VT, XT>(P, 1, x, s0, s1);
+      if (kb < e) {
+        pair_accumulate<ROW0, VT, XT>(Q, 0, x, s0, s1);
+        if (kb + 1 < e) pair_accumulate<ROW0, VT, XT>(Q, 1, x, s0, s1);
       }
     }
   }

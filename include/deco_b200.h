@@ -137,6 +137,12 @@ int deco_fsai_apply(deco_ctx ctx, deco_fsai F, const double* d_x, double* d_y);
  * capture.  Calls that overlap on the GPU (several streams at once) race on the
  * array.  Has no counterpart in the reference. */
 int deco_fsai_apply_static(deco_ctx ctx, deco_fsai F, const double* d_x, double* d_y);
+/* y = FU^T (FL x) with float32 vectors, for a factor made with precision 32:
+ * the product a mixed-precision CPR applies inside its own preconditioner
+ * (float32 values, float32 intermediate).  d_x may equal d_y.  A precision-64
+ * factor returns DECO_ERR_ARG.  Has no counterpart in the reference (its FSAI
+ * works in double only). */
+int deco_fsai_apply_f32(deco_ctx ctx, deco_fsai F, const float* d_x, float* d_y);
 
 /* -------------------------------------------------------------------- CPR
  * CPR<int,int,double,Mglobal,Mlocal>(const ptree& prec, shared_ptr<CSR> A, V*& b)

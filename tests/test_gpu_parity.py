@@ -116,6 +116,27 @@ def test_fsai_matches_reference(d, oracle, name, tols, power):
     assert rel(F.apply(cuda(x)).cpu().numpy(), R.apply(x)) < 1e-12
 
 
+@pytest.mark.parametrize("name", ["c1", "bs3_faults"])
+def test_fsai_apply_f32(d, oracle, name):
+    """Float32 vectors through a precision-32 factor (the product the mixed CPR
+    applies): within 1e-5 of the reference's float64 FSAI::apply on the same
+    float32-rounded input; in place; a precision-64 factor is refused."""
+    _, ref = oracle
+    s = system(name)
+    A = d.CSR.from_system(s)
+    F = d.FSAI({"tol_rel": 0.0, "tol_abs": 0.0, "power": 1}, A, precision=32)
+    x32 = np.random.default_rng(8).standard_normal(s.n).astype(np.float32)
+    y = F.apply_f32(cuda(x32))
+    assert y.dtype == torch.float32
+    R = ref.Fsai(s.r, s.c, s.v, 0.0, 0.0, 1)
+    assert rel(y.cpu().numpy().astype(np.float64), R.apply(x32.astype(np.float64))) < 1e-5
+    xx = cuda(x32)
+    F.apply_f32(xx, xx)
+    assert torch.equal(xx, y)
+    with pytest.raises(d.DecoError):
+        d.FSAI({"tol_rel": 0.0, "tol_abs": 0.0, "power": 1}, A).apply_f32(cuda(x32))
+
+
 def test_fsai_apply_in_place(d, oracle):
     s = system("tiny")
     A = d.CSR.from_system(s)
