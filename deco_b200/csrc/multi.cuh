@@ -103,8 +103,11 @@ struct MMGate {
 };
 
 // ------------------------------------------------------------ the kernel
+// Register cap: three resident blocks per SM for 1x1 and 2x2 blocks (80
+// registers; the K = 8 float32 runs otherwise take 82 and fall to two blocks,
+// 38 % slower), two for 3x3 blocks (whose K = 8 sums need more).
 template <int SW, int BS, int K, bool ROW0, typename VT, typename XT, class Epi>
-__global__ void __launch_bounds__(256) bsr_mm_kernel(int nbr, const int* __restrict__ br, const int* __restrict__ bc,
+__global__ void __launch_bounds__(256, BS > 2 ? 2 : 3) bsr_mm_kernel(int nbr, const int* __restrict__ br, const int* __restrict__ bc,
                                                      const VT* __restrict__ bv, long long plane,
                                                      const XT* __restrict__ x, Epi epi, MMGate gate) {
   constexpr int NR = ROW0 ? 1 : BS;
