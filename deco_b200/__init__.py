@@ -425,7 +425,9 @@ class CPR:
 
 class SOL:
     """SOL<R,C,V>(sol, A, precond, b, x) of solver/SOL.hpp:19-39: the solve runs in
-    the constructor; results in x, iter, res_abs, res_rel, flag (+ resvec)."""
+    the constructor; results in x, iter, res_abs, res_rel, flag (+ resvec), and
+    res_rel_orig, the relative residual of the original system before the CPR
+    decoupling (res_rel is on the decoupled system, as in the reference)."""
 
     def __init__(self, sol: dict, A: CSR, precond: CPR | None, b, x=None, precision: int = 64):
         torch = _torch()
@@ -439,6 +441,7 @@ class SOL:
                                      _ptr(self.x), C.byref(self.params), C.byref(res), self.resvec.ctypes.data))
         self.iter, self.flag = res.iter, res.flag
         self.res_abs, self.res_rel = res.res_abs, res.res_rel
+        self.res_rel_orig = res.res_rel_orig
         self.time_ms, self.restarts = res.t_solve_ms, res.restarts
         self.phases_ms = {"precond": res.t_precond_ms, "matvec": res.t_matvec_ms, "ortho": res.t_ortho_ms}
         self.resvec = self.resvec[: self.iter]
@@ -476,6 +479,7 @@ class ADJ:
                                        self.resvec.ctypes.data))
         self.iter, self.flag = res.iter, res.flag
         self.res_abs, self.res_rel = res.res_abs, res.res_rel
+        self.res_rel_orig = res.res_rel_orig
         self.time_ms = res.t_solve_ms
         self.resvec = self.resvec[: self.iter]
         return lam

@@ -14,6 +14,9 @@
 // vector work: restriction r[s*bs+p] - (A x)[s*bs], prolongation
 // x[s*bs+p] += xp, residual r - A x, and the final x += FSAI(rt) accumulate
 // straight into x, so rt is never written back.
+#include <cmath>
+#include <vector>
+
 #include "cpr.cuh"
 
 namespace deco {
@@ -331,6 +334,62 @@ __global__ void cpr_decouple_rhs(int sn, int bs, int weights, int use_drs, int c
   }
 }
 
+// e_k: 1 in row k of every cell, 0 elsewhere (column k of I, per cell)
+__global__ void cpr_unit_column(long long n, int bs, int k, double* __restrict__ e) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    e[i] = (i % bs == k) ? 1.0 : 0.0;
+}
+
+// Per cell: T (column k = T e_k, from Tk), y = T^-1 r and z = T^-1 b by Gaussian
+// elimination with partial pivoting; per-block sums of |y|^2 and |z|^2 in a fixed
+// order (part[blockIdx.x], part[gridDim.x + blockIdx.x]).
+__global__ void cpr_undecoupled_norms(int sn, int bs, const double* __restrict__ T0, const double* __restrict__ T1,
+                                      const double* __restrict__ T2, const double* __restrict__ r,
+                                      const double* __restrict__ b, double* __restrict__ part) {
+  double sr = 0.0, sb = 0.0;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < sn; s += gridDim.x * blockDim.x) {
+    const long long i0 = (long long)s * bs;
+    double M[3][5];
+    const double* Tk[3] = {T0, T1, T2};
+    for (int i = 0; i < bs; ++i) {
+      for (int k = 0; k < bs; ++k) M[i][k] = Tk[k][i0 + i];
+      M[i][bs] = r[i0 + i];
+      M[i][bs + 1] = b[i0 + i];
+    }
+    bool singular = false;
+    for (int c = 0; c < bs; ++c) {
+      int piv = c;
+      for (int i = c + 1; i < bs; ++i)
+        if (fabs(M[i][c]) > fabs(M[piv][c])) piv = i;
+      if (M[piv][c] == 0.0) { singular = true; break; }
+      if (piv != c)
+        for (int k = 0; k < bs + 2; ++k) { const double t = M[c][k]; M[c][k] = M[piv][k]; M[piv][k] = t; }
+      for (int i = 0; i < bs; ++i) {
+        if (i == c) continue;
+        const double f = M[i][c] / M[c][c];
+        for (int k = c; k < bs + 2; ++k) M[i][k] -= f * M[c][k];
+      }
+    }
+    if (singular) { sr = NAN; continue; }
+    for (int i = 0; i < bs; ++i) {
+      const double y = M[i][bs] / M[i][i], z = M[i][bs + 1] / M[i][i];
+      sr += y * y;
+      sb += z * z;
+    }
+  }
+  __shared__ double ps[2][32];
+  sr = warp_sum(sr);
+  sb = warp_sum(sb);
+  if ((threadIdx.x & 31) == 0) { ps[0][threadIdx.x >> 5] = sr; ps[1][threadIdx.x >> 5] = sb; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, c = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { a += ps[0][w]; c += ps[1][w]; }
+    part[blockIdx.x] = a;
+    part[gridDim.x + blockIdx.x] = c;
+  }
+}
+
 __global__ void unfix_diag(int n, const int* __restrict__ r, const int* __restrict__ c, double* __restrict__ v,
                            const char* __restrict__ chk) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -560,6 +619,33 @@ void cpr_apply32(deco_ctx_s* ctx, deco_cpr_s* P, const RT* r, XT* x) {
   if (P->prm.seq == 0) return;
   spmv<float, XT>(ctx, A, x, EpiResid<RT, float>{r, P->rt32.get()});
   glo_stage<float, float, float>(ctx, P, P->rt32.get(), tg, EpiAdd<XT>{x}, true);
+}
+
+double cpr_original_relres(deco_ctx_s* ctx, deco_cpr_s* P, const double* r, const double* b) {
+  cudaStream_t st = ctx->stream;
+  const int bs = P->bs;
+  const long long n = P->n;
+  const deco_cpr_params& m = P->prm;
+  DevBuf<double> Tk[3];
+  for (int k = 0; k < bs; ++k) {
+    Tk[k].alloc(n, st);
+    cpr_unit_column<<<grid_for(ctx, n, 256), 256, 0, st>>>(n, bs, k, Tk[k].get());
+    DECO_CHECK_LAUNCH();
+    cpr_decouple_rhs<<<grid_for(ctx, P->sn, 256), 256, 0, st>>>(P->sn, bs, m.weights, m.use_drs, m.cpd, P->w0.get(),
+                                                                P->ops.get(), P->J.get(), Tk[k].get());
+    DECO_CHECK_LAUNCH();
+  }
+  const int grid = grid_for(ctx, P->sn, 256);
+  DevBuf<double> part(2 * (size_t)grid, st);
+  cpr_undecoupled_norms<<<grid, 256, 0, st>>>(P->sn, bs, Tk[0].get(), bs > 1 ? Tk[1].get() : nullptr,
+                                              bs > 2 ? Tk[2].get() : nullptr, r, b, part.get());
+  DECO_CHECK_LAUNCH();
+  std::vector<double> h(2 * (size_t)grid);
+  DECO_CUDA(cudaMemcpyAsync(h.data(), part.get(), sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
+  DECO_CUDA(cudaStreamSynchronize(st));
+  double sr = 0.0, sb = 0.0;
+  for (int i = 0; i < grid; ++i) { sr += h[i]; sb += h[grid + i]; }
+  return std::sqrt(sr) / std::sqrt(sb);
 }
 
 template void cpr_apply32<double, double>(deco_ctx_s*, deco_cpr_s*, const double*, double*);

@@ -26,6 +26,13 @@ namespace deco {
 // x = M^{-1} r, float64 preconditioner (apply_seq0/1/3, precond/CPR.hpp:176-299).
 void cpr_apply64(deco_ctx_s* ctx, deco_cpr_s* P, const double* r, double* x);
 
+// ||T^-1 r|| / ||T^-1 b|| for the block-diagonal decoupling T that the CPR setup
+// applied to the system (row swaps, weights, DRS, IMPES sum, CPD), r and b given
+// in the decoupled form: the relative residual of the original system.  T's
+// blocks are recovered by replaying the decoupling on unit vectors; NaN if a
+// block is singular.  Synchronises the context's stream.
+double cpr_original_relres(deco_ctx_s* ctx, deco_cpr_s* P, const double* r, const double* b);
+
 // x = M^{-1} r with float32 factors, float32 A copy and float32 internal vectors;
 // r and x may be float64 or float32.
 template <typename RT, typename XT>

@@ -761,6 +761,10 @@ struct Solver {
     res->t_precond_ms = t_phase[0];
     res->t_matvec_ms = t_phase[1];
     res->t_ortho_ms = t_phase[2];
+    // the residual of the original (not decoupled) system: b - A x on the
+    // decoupled system, mapped back through the inverse of the CPR's decoupling
+    spmv<double, double>(ctx, A, x, EpiResid<double, double>{b, xtmp.get()});
+    res->res_rel_orig = P ? cpr_original_relres(ctx, P, xtmp.get(), b) : norm2(xtmp.get()) / norm2(b);
     if (prm.verbosity > 0) {
       std::printf("\n--------------------------------\n");
       std::printf("Profile of %s:\n", left ? "lGMRES" : "rGMRES");

@@ -180,6 +180,7 @@ int main(int argc, char** argv) {
     std::printf("Profile of %s:\n", param.get<std::string>("sol.type") == "lgmres" ? "lGMRES" : "rGMRES");
     std::printf("iteration count =  %d\n", S->iter);
     std::printf("residual = %.2e\n", S->res_rel);
+    std::printf("residual of the original system = %.2e\n", S->res_rel_orig);
     auto t = P->timings();
     std::printf("\nprofile (s)\n");
     std::printf("  setup & solve       %10.5f\n", t_prec + t_sol);

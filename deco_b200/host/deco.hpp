@@ -278,6 +278,7 @@ class SOL {
   V* x;
   int iter = 0;
   double res_abs = 0, res_rel = 0;
+  double res_rel_orig = 0;  // original (not decoupled) system; res_rel is on the decoupled one
   int flag = 1;
   double time_ms = 0;
   std::vector<double> resvec;
@@ -314,6 +315,7 @@ class SOL {
     flag = res.flag;
     res_abs = res.res_abs;
     res_rel = res.res_rel;
+    res_rel_orig = res.res_rel_orig;
     time_ms = res.t_solve_ms;
     resvec.resize(iter);
   }

@@ -223,6 +223,10 @@ typedef struct deco_sol_result {
    * Arnoldi steps spent in the preconditioner, in the SpMV with A, and in the
    * orthogonalisation (0 otherwise) */
   double t_precond_ms, t_matvec_ms, t_ortho_ms;
+  /* ||b0 - A0 x|| / ||b0|| for the ORIGINAL system A0 x = b0, before the CPR
+   * decoupling rewrote A and b (res_rel is on the decoupled system, as the
+   * reference reports it).  Equals the true relative residual when P is NULL. */
+  double res_rel_orig;
 } deco_sol_result;
 
 /* Solves A x = b with preconditioner P (NULL: identity).  A and d_b are the

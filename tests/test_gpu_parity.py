@@ -290,6 +290,37 @@ def test_gmres_mixed_precision_reaches_fp64_residual(d, oracle):
     assert S.iter <= 2 * ref_it
 
 
+ORIG_CASES = {
+    "ge_cpd_bs2": ("c1", dict(), "rgmres", 64),
+    "drs_bs2_mixed": ("c1", dict(drs=1, e_ps=0.05), "rgmres", 32),
+    "qimpes_bs3_lgmres": ("bs3_faults", dict(weights="quasiimpes"), "lgmres", 64),
+    "ge_bs3_no_cpd": ("bs3_faults", dict(cpd=0), "rgmres", 64),
+}
+
+
+@pytest.mark.parametrize("name", list(ORIG_CASES))
+def test_gmres_reports_original_system_residual(d, oracle, name):
+    """res_rel is on the decoupled system (as the reference reports it); res_rel_orig
+    is ||b0 - A0 x|| / ||b0|| on the system before the CPR setup rewrote A and b,
+    checked here against the original arrays on the CPU: within 1e-12 of ||b0||
+    (forming b - A x at a residual of 1e-8 cancels eight digits, so both sides
+    carry rounding of that size) plus 1e-6 relative."""
+    port, _ = oracle
+    sysname, kw, stype, precision = ORIG_CASES[name]
+    s = system(sysname)
+    A = d.CSR.from_system(s)
+    b = cuda(s.b)
+    P = d.CPR(cpr_json(s.bs, **kw), A, b, precision=precision)
+    S = d.SOL(sol_json(type_=stype), A, P, b, precision=precision)
+    assert S.flag == 0
+    x = S.x.cpu().numpy()
+    orig = np.linalg.norm(s.b - port.spmv(s.r, s.c, s.v, x)) / np.linalg.norm(s.b)
+    assert abs(S.res_rel_orig - orig) <= 1e-6 * orig + 1e-12, (S.res_rel_orig, orig)
+    # without a preconditioner the solve has no decoupling to undo: the two agree
+    S0 = d.SOL(sol_json(itmax=5), A, None, b)
+    assert abs(S0.res_rel_orig - S0.res_rel) <= 1e-12 * S0.res_rel
+
+
 def test_gmres_no_preconditioner_and_x0(d):
     s = gen.grid(3, 3, 3, bs=2, seed=5)  # 54 rows: GMRES(60) is full GMRES
     A = d.CSR.from_system(s)
