@@ -507,7 +507,8 @@ def main():
             return nblk * 4 + nblk * bsz * bsz * vb + 4 * (n // bsz + 1)
         return nz * (4 + vb) + 4 * (n + 1)
 
-    fmt = "cell-block (bs %d)" % A.blocks[0] if A.blocks[0] else "CSR"
+    fmt = ("cell-block (bs %d)" % A.blocks[0] if A.blocks[0] else "CSR") + \
+        (", %d padded slots per cell" % A.padded if A.padded else "")
     ms = kernel_ms(lambda: A.apply_f32(x32, y32))
     alg32 = matrix_bytes(nnz, A.blocks, 4) + 4 * n + 4 * n
     kernels["spmv_A_f32"] = {"ms": ms, "gbs": alg32 / ms / 1e6, "alg_bytes": alg32, "format": fmt,
@@ -519,7 +520,9 @@ def main():
     ms = kernel_ms(lambda: Fg.apply(x64, y64))
     algF = matrix_bytes(nzF, (fb, kl), 8) + matrix_bytes(nzF, (fb, ku), 8) + 8 * n + 2 * 8 * n + 8 * n
     kernels["fsai_apply_global_f64"] = {"ms": ms, "gbs": algF / ms / 1e6, "alg_bytes": algF, "nnz_factor": nzF,
-                                        "format": "cell-block (bs %d)" % fb if fb else "CSR"}
+                                        "format": ("cell-block (bs %d)" % fb if fb else "CSR")
+                                        + (", %d/%d padded slots" % Fg.padded if Fg.padded[0] else ""),
+                                        "note": "the intermediate FL x (64 MB) stays in L2 between the two products"}
     del P64
     P32 = d.CPR(PREC, d.CSR(n, n, r_d, c_d, v_d, ctx), b_d.clone(), precision=32)
     Fg32 = P32.fsai(0)
@@ -542,13 +545,19 @@ def main():
     dom = kernels["spmv_A_f32"]
     roofline = {"bound": "hbm", "achieved": dom["gbs"], "peak": peak, "unit": "GB/s", "frac": dom["gbs"] / peak,
                 # DRAM read + write bytes per launch of this kernel from one ncu capture of this
-                # workload (profiles/bsr2_pair_f32_config3_full.md): 604.8 MB read + 11.5 MB written
-                "traffic": 616.3e6 if A.blocks[0] == 2 else None,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/bsr2_pair_f32_config3_full.md"
+                # workload: the padded kernel 672.0 MB read + 8.9 MB written
+                # (profiles/ell2_f32_config3_full.md); the pair kernel 604.8 + 11.5 MB
+                # (profiles/bsr2_pair_f32_config3_full.md)
+                "traffic": (680.9e6 if A.padded == 8 else 616.3e6 if A.blocks[0] == 2 and not A.padded else None),
+                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/"
+                                   + ("ell2_f32_config3_full.md" if A.padded else "bsr2_pair_f32_config3_full.md"))
                 if A.blocks[0] == 2 else None,
-                "kernel": {2: "deco::bsr2_pair_kernel<float> (2x2 cell blocks)",
-                           3: "deco::bsr_kernel<float> (3x3 cell blocks)"}.get(A.blocks[0], "deco::spmv_kernel<float> (CSR)")
+                "kernel": ("deco::ell2_kernel<%d, float> (2x2 cell blocks, %d padded slots per cell)" % (A.padded, A.padded)
+                           if A.padded else
+                           {2: "deco::bsr2_pair_kernel<float> (2x2 cell blocks)",
+                            3: "deco::bsr_kernel<float> (3x3 cell blocks)"}.get(A.blocks[0], "deco::spmv_kernel<float> (CSR)"))
                 + " on A (8M rows, 111.36M nnz, float32 values)",
+                "algorithmic_bytes": "the unpadded cell-block layout's bytes (padding slots count against the kernel)",
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind}
 
     cpu = None

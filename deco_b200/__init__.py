@@ -194,6 +194,13 @@ class CSR:
         check(lib().deco_csr_blocks(self.h, C.byref(b), C.byref(k)))
         return b.value, k.value
 
+    @property
+    def padded(self):
+        """Slots per cell of the padded 2x2-block copy the products use (4 or 8; 0: none)."""
+        w = C.c_int()
+        check(lib().deco_csr_padded(self.h, C.byref(w)))
+        return w.value
+
     def transpose(self) -> "CSR":
         """A^T on the device, rows in ascending column order."""
         h = C.c_void_p()
@@ -265,6 +272,13 @@ class FSAI:
             b = torch.empty(self.n, dtype=torch.float32, device="cuda")
         check(lib().deco_fsai_apply_f32(self.ctx.h, self.h, _ptr(x), _ptr(b)))
         return b
+
+    @property
+    def padded(self):
+        """(slots of FL's, slots of FU^T's) padded 2x2-block copies: 4 or 8, 0 without."""
+        a, b = C.c_int(), C.c_int()
+        check(lib().deco_fsai_padded(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     @property
     def blocks(self):

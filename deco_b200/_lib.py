@@ -63,6 +63,7 @@ SIGNATURES = {
     "deco_csr_set_subwarp": ([vp, C.c_int], C.c_int),
     "deco_csr_set_blocks": ([vp, vp, C.c_int], C.c_int),
     "deco_csr_blocks": ([vp, ip, ip], C.c_int),
+    "deco_csr_padded": ([vp, ip], C.c_int),
     "deco_spmv": ([vp, vp, vp, vp, C.c_int], C.c_int),
     "deco_spmv_f32": ([vp, vp, vp, vp, C.c_int], C.c_int),
     "deco_residual": ([vp, vp, vp, vp, vp], C.c_int),
@@ -72,6 +73,7 @@ SIGNATURES = {
     "deco_fsai_blocks": ([vp, ip, ip, ip], C.c_int),
     "deco_fsai_download": ([vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
     "deco_fsai_apply": ([vp, vp, vp, vp], C.c_int),
+    "deco_fsai_padded": ([vp, ip, ip], C.c_int),
     "deco_fsai_apply_f32": ([vp, vp, vp, vp], C.c_int),
     "deco_fsai_apply_static": ([vp, vp, vp, vp], C.c_int),
     "deco_cpr_create": ([vp, vp, vp, C.POINTER(CprParams), C.POINTER(vp)], C.c_int),

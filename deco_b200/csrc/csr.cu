@@ -71,6 +71,55 @@ __global__ void bsr_fill(int nbr, int bs, const int* __restrict__ r, const int* 
 
 }  // namespace
 
+// slot-major padded values (and columns when ec != nullptr) from the block planes
+template <typename T>
+__global__ void ell2_fill(int nbr, int W, const int* __restrict__ br, const int* __restrict__ bc,
+                          const T* __restrict__ bv, long long plane, int* __restrict__ ec, T* __restrict__ ev) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nbr; s += gridDim.x * blockDim.x) {
+    const int a = br[s], e = br[s + 1];
+    for (int k = 0; k < W; ++k) {
+      const bool on = a + k < e;
+      // an unused slot reads a column the cell already has (or column 0) with zero values
+      if (ec) ec[(long long)k * nbr + s] = on ? bc[a + k] : (e > a ? bc[a] : 0);
+      for (int q = 0; q < 2; ++q)
+        for (int t = 0; t < 2; ++t)
+          ev[2 * ((long long)(q * W + k) * nbr + s) + t] = on ? bv[q * plane + 2LL * (a + k) + t] : (T)0;
+    }
+  }
+}
+
+void make_padded(deco_ctx_s* ctx, deco_csr_s* A) {
+  cudaStream_t st = ctx->stream;
+  const int nbr = A->n / 2;
+  if (!A->ew) {
+    if (!ctx->padded || A->bbs != 2 || nbr <= 0 || A->m < 2) return;
+    DevBuf<int> mx(1, st);
+    mx.zero(st);
+    row_stats<<<grid_for(ctx, nbr, 256), 256, 0, st>>>(A->br.get(), nbr, mx.get());
+    DECO_CHECK_LAUNCH();
+    int maxb = 0;
+    DECO_CUDA(cudaMemcpyAsync(&maxb, mx.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+    DECO_CUDA(cudaStreamSynchronize(st));
+    int W = 0;
+    if (maxb <= 4) W = 4;
+    else if (maxb <= 8 && 8.0 * nbr <= 1.25 * A->nblk) W = 8;
+    if (!W) return;
+    A->ew = W;
+    A->ec.alloc((size_t)W * nbr, st);
+    A->ev.alloc((size_t)4 * W * nbr, st);
+    ell2_fill<double><<<grid_for(ctx, nbr, 256), 256, 0, st>>>(nbr, W, A->br.get(), A->bc.get(), A->bv.get(),
+                                                               A->bplane, A->ec.get(), A->ev.get());
+    DECO_CHECK_LAUNCH();
+  }
+  if (A->bv32) {
+    const int W = A->ew;
+    if (!A->ev32 || A->ev32.size() != (size_t)4 * W * nbr) A->ev32.alloc((size_t)4 * W * nbr, st);
+    ell2_fill<float><<<grid_for(ctx, nbr, 256), 256, 0, st>>>(nbr, W, A->br.get(), A->bc.get(), A->bv32.get(),
+                                                              A->bplane, nullptr, A->ev32.get());
+    DECO_CHECK_LAUNCH();
+  }
+}
+
 void drop_bsr(deco_csr_s* A) {
   A->bbs = 0;
   A->nblk = 0;
@@ -80,6 +129,10 @@ void drop_bsr(deco_csr_s* A) {
   A->bv = DevBuf<double>();
   A->bv32 = DevBuf<float>();
   A->bsw64 = A->bsw32 = 0;
+  A->ew = 0;
+  A->ec = DevBuf<int>();
+  A->ev = DevBuf<double>();
+  A->ev32 = DevBuf<float>();
 }
 
 void make_bsr(deco_ctx_s* ctx, deco_csr_s* A, int bs, double max_fill) {
@@ -111,6 +164,7 @@ void make_bsr(deco_ctx_s* ctx, deco_csr_s* A, int bs, double max_fill) {
     to_f32<<<grid_for(ctx, plane * bs, 256), 256, 0, st>>>(A->bv.get(), A->bv32.get(), plane * bs);
     DECO_CHECK_LAUNCH();
   }
+  make_padded(ctx, A);
 }
 
 void refresh_stats(deco_ctx_s* ctx, deco_csr_s* A) {
@@ -134,6 +188,7 @@ void make_f32_values(deco_ctx_s* ctx, deco_csr_s* A) {
     if (!A->bv32 || A->bv32.size() != (size_t)nv) A->bv32.alloc(nv, ctx->stream);
     to_f32<<<grid_for(ctx, nv, 256), 256, 0, ctx->stream>>>(A->bv.get(), A->bv32.get(), nv);
     DECO_CHECK_LAUNCH();
+    if (A->ew) make_padded(ctx, A);
   }
 }
 
@@ -355,6 +410,13 @@ int deco_csr_blocks(deco_csr A, int* bs, int* nblk) {
     DECO_REQUIRE(A, DECO_ERR_ARG, "A is NULL");
     if (bs) *bs = A->bbs;
     if (nblk) *nblk = A->nblk;
+  });
+}
+
+int deco_csr_padded(deco_csr A, int* slots) {
+  return guard([&] {
+    DECO_REQUIRE(A && slots, DECO_ERR_ARG, "NULL argument");
+    *slots = A->ew;
   });
 }
 

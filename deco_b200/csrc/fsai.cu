@@ -765,6 +765,14 @@ int deco_fsai_blocks(deco_fsai F, int* bs, int* nblk_lower, int* nblk_upper) {
   });
 }
 
+int deco_fsai_padded(deco_fsai F, int* slots_lower, int* slots_upper) {
+  return guard([&] {
+    DECO_REQUIRE(F, DECO_ERR_ARG, "F is NULL");
+    if (slots_lower) *slots_lower = F->FL.ew;
+    if (slots_upper) *slots_upper = F->FUt.ew;
+  });
+}
+
 int deco_fsai_download(deco_ctx ctx, deco_fsai F, int* Lr, int* Lc, double* Lv, int* Ur, int* Uc, double* Uv) {
   int rc = deco_csr_download(ctx, &F->FL, Lr, Lc, Lv);
   if (rc) return rc;

@@ -44,6 +44,8 @@ def test_block_products_match_oracle(d, name):
     A.set_blocks(s.bs)
     bs, nblk = A.blocks
     assert bs == s.bs and nblk * bs * bs == s.nnz  # generated systems are dense cell blocks
+    # 7-point cells carry up to 7 blocks: 8 padded slots when that pads at most 25 %
+    assert A.padded == (8 if bs == 2 and 8 * (s.n // 2) <= 1.25 * nblk else 0)
     x = np.random.default_rng(0).standard_normal(s.n)
     assert rel(A.apply(cuda(x)).cpu().numpy(), port.spmv(s.r, s.c, s.v, x)) < 1e-12
     assert rel(A.apply(cuda(x), bs=s.bs).cpu().numpy(), port.spmv(s.r, s.c, s.v, x, s.bs)) < 1e-12
@@ -55,6 +57,38 @@ def test_block_products_match_oracle(d, name):
     assert rel(A.apply(xx[1:]).cpu().numpy(), port.spmv(s.r, s.c, s.v, x)) < 1e-12
     A.set_blocks(0)
     assert A.blocks == (0, 0)
+
+
+def test_padded_copy_products(d):
+    """The slot-padded 2x2 copy (products of matrices with at most 4 blocks per
+    cell, as the FSAI factors of 7-point systems): a rectangular matrix with empty
+    cells and 0-4 blocks per cell; full, row-0 and float32 products against the
+    oracle; unused slots read a valid column with zero values."""
+    from oracle import port
+    rng = np.random.default_rng(9)
+    ncell, mcell = 500, 300
+    rows, cols = [], []
+    for s_ in range(ncell):
+        cs = np.sort(rng.choice(mcell, int(rng.integers(0, 5)), replace=False))
+        for i in range(2):
+            for c_ in cs:
+                rows += [2 * s_ + i] * 2
+                cols += [2 * c_, 2 * c_ + 1]
+    rows, cols = np.array(rows), np.array(cols, dtype=np.int32)
+    r = np.zeros(2 * ncell + 1, np.int32)
+    np.cumsum(np.bincount(rows, minlength=2 * ncell), out=r[1:])
+    v = rng.standard_normal(len(cols))
+    A = d.CSR(2 * ncell, 2 * mcell, r, cols, v)
+    A.set_blocks(2)
+    assert A.blocks[0] == 2 and A.padded == 4
+    x = rng.standard_normal(2 * mcell)
+    assert rel(A.apply(cuda(x)).cpu().numpy(), port.spmv(r, cols, v, x)) < 1e-12
+    assert rel(A.apply(cuda(x), bs=2).cpu().numpy(), port.spmv(r, cols, v, x, 2)) < 1e-12
+    y32 = A.apply_f32(cuda(x.astype(np.float32))).cpu().numpy()
+    assert rel(y32, port.spmv(r, cols, v.astype(np.float32).astype(np.float64),
+                              x.astype(np.float32).astype(np.float64))) < 1e-6
+    A.set_blocks(0)
+    assert A.padded == 0
 
 
 def test_padding_with_zeros(d):
@@ -98,6 +132,8 @@ def test_cpr_builds_blocks_and_keeps_parity(d, precision):
     P = d.CPR(prec, A, b, precision)
     assert A.blocks[0] == 2
     assert P.fsai(0).n == s.n
+    # power-1 factors of a 7-point system: at most 4 blocks per cell -> 4 padded slots
+    assert P.fsai(0).padded == (4, 4)
     O = port.Cpr(prec, s.r, s.c, s.v, s.b)
     rvec = np.random.default_rng(5).standard_normal(s.n)
     tol = 1e-12 if precision == 64 else 1e-5
