@@ -172,6 +172,78 @@ __global__ void __launch_bounds__(256, BS > 2 ? 2 : 3) bsr_mm_kernel(int nbr, co
       if ((q * K + k) % SW == lane) epi(ROW0 ? s : s * BS + q, k, acc[q][k]);
 }
 
+// K-column product of a 2x2-block matrix with a slot-padded copy (see
+// ell2_kernel): one thread per cell holds the cell's 2 x K sums, walks its W
+// slots (column, two values per plane, the K values of the two x rows it
+// multiplies) and writes its outputs; no row pointer, no sub-warp reduction.
+// The block rows sum in slot order as in the single-vector padded product.
+template <int W, int K, bool ROW0, typename VT, typename XT, class Epi>
+__global__ void __launch_bounds__(256, 3) ell2_mm_kernel(int nbr, const int* __restrict__ ec,
+                                                         const VT* __restrict__ ev, const XT* __restrict__ x, Epi epi,
+                                                         MMGate gate) {
+  constexpr int NR = ROW0 ? 1 : 2;
+  using V2 = typename Pair<VT>::V;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nbr) return;
+  if (gate.active && __ldg(gate.active + __ldg(gate.cell_sys + s / gate.div)) == 0) return;
+  const V2* __restrict__ e2 = reinterpret_cast<const V2*>(ev);
+  double acc[NR][K];
+#pragma unroll
+  for (int q = 0; q < NR; ++q)
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[q][k] = 0.0;
+#pragma unroll 2
+  for (int j = 0; j < W; ++j) {
+    const long long o = (long long)__ldcs(ec + (long long)j * nbr + s) * 2 * K;  // x rows 2c, 2c+1
+    const V2 a = __ldcs(e2 + (long long)j * nbr + s);
+    V2 b = a;
+    if (!ROW0) b = __ldcs(e2 + (long long)(W + j) * nbr + s);
+    if constexpr (kRunF32<VT, XT>) {
+      float x0[K], x1[K];
+      load_k_f32<K>(x, o, x0);
+      load_k_f32<K>(x, o + K, x1);
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        acc[0][k] += (double)fmaf(a.y, x1[k], a.x * x0[k]);
+        if (!ROW0) acc[NR - 1][k] += (double)fmaf(b.y, x1[k], b.x * x0[k]);
+      }
+    } else {
+      double x0[K], x1[K];
+      load_k<K, XT>(x, o, x0);
+      load_k<K, XT>(x, o + K, x1);
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        acc[0][k] += (double)a.x * x0[k];
+        acc[0][k] += (double)a.y * x1[k];
+        if (!ROW0) {
+          acc[NR - 1][k] += (double)b.x * x0[k];
+          acc[NR - 1][k] += (double)b.y * x1[k];
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < NR; ++q)
+#pragma unroll
+    for (int k = 0; k < K; ++k) epi(ROW0 ? s : 2 * s + q, k, acc[q][k]);
+}
+
+template <int K, typename VT, typename XT, class Epi>
+void launch_ell2_mm(cudaStream_t st, const deco_csr_s* A, const VT* ev, bool row0, const XT* x, Epi epi,
+                    MMGate gate) {
+  const int nbr = A->n / 2;
+  if (nbr <= 0) return;
+  const unsigned grid = (unsigned)cdiv(nbr, 256);
+  if (A->ew == 4) {
+    if (row0) ell2_mm_kernel<4, K, true, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, gate);
+    else ell2_mm_kernel<4, K, false, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, gate);
+  } else {
+    if (row0) ell2_mm_kernel<8, K, true, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, gate);
+    else ell2_mm_kernel<8, K, false, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, gate);
+  }
+  DECO_CHECK_LAUNCH();
+}
+
 // A matrix for the K-column product: its cell-block copy when it has one
 // (BS = bbs), else the CSR arrays as BS = 1 blocks.
 struct MMView {
@@ -234,6 +306,14 @@ void spmm(deco_ctx_s* ctx, const deco_csr_s* A, const XT* x, Epi epi, bool row0 
     else gate = MMGate{};
   }
   cudaStream_t st = ctx->stream;
+  if (M.bs == 2 && A->ew) {
+    const VT* ev;
+    if constexpr (sizeof(VT) == 4) ev = A->ev32.get(); else ev = A->ev.get();
+    if (ev) {
+      launch_ell2_mm<K, VT, XT, Epi>(st, A, ev, row0, x, epi, gate);
+      return;
+    }
+  }
   if (M.bs == 1) launch_mm_bs<1, K, false, VT, XT, Epi>(st, M, v, x, epi, gate);
   else if (M.bs == 2) {
     if (row0) launch_mm_bs<2, K, true, VT, XT, Epi>(st, M, v, x, epi, gate);
