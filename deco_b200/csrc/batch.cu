@@ -198,6 +198,18 @@ __device__ __forceinline__ void vload(const T* __restrict__ p, double* o, bool s
     for (int q = 0; q < E; ++q) o[q] = (double)e[q];
   }
 }
+template <int E>
+__device__ __forceinline__ void vload_f32(const float* __restrict__ p, float* o, bool stream) {
+  using V = typename VecN<float, E>::t;
+  const V v = stream ? __ldcs(reinterpret_cast<const V*>(p)) : __ldg(reinterpret_cast<const V*>(p));
+  if constexpr (E == 1) {
+    o[0] = v;
+  } else {
+    const float* e = reinterpret_cast<const float*>(&v);
+#pragma unroll
+    for (int q = 0; q < E; ++q) o[q] = e[q];
+  }
+}
 template <typename T, int E>
 __device__ __forceinline__ void vstore(T* p, const T* o) {
   using V = typename VecN<T, E>::t;
@@ -253,19 +265,58 @@ __global__ void __launch_bounds__(kT) b_dots_v(const int* crow, const int* csys,
   for (int t = 0; t < NS; ++t) acc[t] = 0.0;
   if (live) {
     const T* __restrict__ uj = V + (long long)j * ld;
-    for (long long f = f0 + threadIdx.x; f < f1; f += kT) {
-      double wv[E], uv[E];
-      vload<T, E>(w + f * E, wv, false);
-      vload<T, E>(uj + f * E, uv, false);
+    if constexpr (std::is_same<T, float>::value) {
+      // float32 basis: a thread's vectors f and f + kT hold the same instances
+      // (kT is a multiple of the phase count), so each instance's two products
+      // are summed in float32 and converted once (no widening of w and u_j, a
+      // quarter of the conversions, two rows' loads in flight per thread)
+      for (long long f = f0 + threadIdx.x; f < f1; f += 2 * kT) {
+        const long long g = f + kT;
+        const bool two = g < f1;
+        float wa[E], ua[E], wb[E], ub[E];
+        vload_f32<E>(w + f * E, wa, false);
+        vload_f32<E>(uj + f * E, ua, false);
+        if (two) {
+          vload_f32<E>(w + g * E, wb, false);
+          vload_f32<E>(uj + g * E, ub, false);
+        } else {
 #pragma unroll
-      for (int t = 0; t < G; ++t) {
-        if (t < ni) {  // uniform over the block
-          double v[E];
-          vload<T, E>(V + (long long)(i0 + t) * ld + f * E, v, true);
+          for (int q = 0; q < E; ++q) { wb[q] = 0.f; ub[q] = 0.f; }
+        }
 #pragma unroll
-          for (int q = 0; q < E; ++q) {
-            acc[t * E + q] += v[q] * wv[q];
-            acc[(G + t) * E + q] += v[q] * uv[q];
+        for (int t = 0; t < G; ++t) {
+          if (t < ni) {  // uniform over the block
+            const float* col = V + (long long)(i0 + t) * ld;
+            float va[E], vb[E];
+            vload_f32<E>(col + f * E, va, true);
+            if (two) vload_f32<E>(col + g * E, vb, true);
+            else {
+#pragma unroll
+              for (int q = 0; q < E; ++q) vb[q] = 0.f;
+            }
+#pragma unroll
+            for (int q = 0; q < E; ++q) {
+              acc[t * E + q] += (double)fmaf(vb[q], wb[q], va[q] * wa[q]);
+              acc[(G + t) * E + q] += (double)fmaf(vb[q], ub[q], va[q] * ua[q]);
+            }
+          }
+        }
+      }
+    } else {
+      for (long long f = f0 + threadIdx.x; f < f1; f += kT) {
+        double wv[E], uv[E];
+        vload<T, E>(w + f * E, wv, false);
+        vload<T, E>(uj + f * E, uv, false);
+#pragma unroll
+        for (int t = 0; t < G; ++t) {
+          if (t < ni) {  // uniform over the block
+            double v[E];
+            vload<T, E>(V + (long long)(i0 + t) * ld + f * E, v, true);
+#pragma unroll
+            for (int q = 0; q < E; ++q) {
+              acc[t * E + q] += v[q] * wv[q];
+              acc[(G + t) * E + q] += v[q] * uv[q];
+            }
           }
         }
       }
