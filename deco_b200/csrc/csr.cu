@@ -120,6 +120,46 @@ void make_padded(deco_ctx_s* ctx, deco_csr_s* A) {
   }
 }
 
+// slot-major padded scalar rows (columns too when ec != nullptr)
+template <typename T>
+__global__ void ell1_fill(int n, int W, const int* __restrict__ r, const int* __restrict__ c, const T* __restrict__ v,
+                          int* __restrict__ ec, T* __restrict__ ev) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int a = r[i], e = r[i + 1];
+    for (int k = 0; k < W; ++k) {
+      const bool on = a + k < e;
+      // an unused slot reads a column the row already has (or column 0) with a zero value
+      if (ec) ec[(long long)k * n + i] = on ? c[a + k] : (e > a ? c[a] : 0);
+      ev[(long long)k * n + i] = on ? v[a + k] : (T)0;
+    }
+  }
+}
+
+void make_padded_scalar(deco_ctx_s* ctx, deco_csr_s* A) {
+  cudaStream_t st = ctx->stream;
+  const int n = A->n;
+  if (!A->ew) {
+    if (!ctx->padded || A->bbs || n <= 0 || A->m < 1) return;
+    int W = 0;
+    if (A->max_row <= 4) W = 4;
+    else if (A->max_row <= 8 && 8.0 * n <= 1.25 * A->nz) W = 8;
+    if (!W) return;
+    A->ew = W;
+    A->ec.alloc((size_t)W * n, st);
+    A->ev.alloc((size_t)W * n, st);
+    ell1_fill<double><<<grid_for(ctx, n, 256), 256, 0, st>>>(n, W, A->r.get(), A->c.get(), A->v.get(), A->ec.get(),
+                                                              A->ev.get());
+    DECO_CHECK_LAUNCH();
+  }
+  if (A->v32) {
+    const int W = A->ew;
+    if (!A->ev32 || A->ev32.size() != (size_t)W * n) A->ev32.alloc((size_t)W * n, st);
+    ell1_fill<float><<<grid_for(ctx, n, 256), 256, 0, st>>>(n, W, A->r.get(), A->c.get(), A->v32.get(), nullptr,
+                                                             A->ev32.get());
+    DECO_CHECK_LAUNCH();
+  }
+}
+
 void drop_bsr(deco_csr_s* A) {
   A->bbs = 0;
   A->nblk = 0;
@@ -177,6 +217,12 @@ void refresh_stats(deco_ctx_s* ctx, deco_csr_s* A) {
   A->avg_row = A->n ? double(A->nz) / A->n : 0.0;
   A->sw64 = A->sw32 = 0;
   A->bsw64 = A->bsw32 = 0;
+  if (!A->bbs && A->ew) {  // a scalar padded copy no longer matches the rows
+    A->ew = 0;
+    A->ec = DevBuf<int>();
+    A->ev = DevBuf<double>();
+    A->ev32 = DevBuf<float>();
+  }
 }
 
 void make_f32_values(deco_ctx_s* ctx, deco_csr_s* A) {
@@ -189,6 +235,8 @@ void make_f32_values(deco_ctx_s* ctx, deco_csr_s* A) {
     to_f32<<<grid_for(ctx, nv, 256), 256, 0, ctx->stream>>>(A->bv.get(), A->bv32.get(), nv);
     DECO_CHECK_LAUNCH();
     if (A->ew) make_padded(ctx, A);
+  } else if (A->ew) {
+    make_padded_scalar(ctx, A);
   }
 }
 

@@ -710,6 +710,9 @@ void fsai_build(deco_ctx_s* ctx, const deco_csr_s* A0, double tol_rel, double to
   if (bs > 1) {
     make_bsr(ctx, &FL, bs);
     make_bsr(ctx, &U, bs);
+  } else {  // (csr_transpose refreshed U's row statistics)
+    make_padded_scalar(ctx, &FL);
+    make_padded_scalar(ctx, &U);
   }
   trace_mark(ctx, "fsai block copies");
   F->tmp.alloc(n, st);

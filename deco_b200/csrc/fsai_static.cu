@@ -19,7 +19,10 @@
 //   * all calls share the array and it keeps the last call's contents; nothing
 //     needs clearing, since the first product writes every entry before the
 //     second reads it;
-//   * calls that overlap on the GPU (two streams at once) race on the array.
+//   * calls that overlap on the GPU (two streams at once) race on the array;
+//   * the two products use the kernels deco_fsai_apply uses whenever those need no
+//     allocation (the padded copies), so the results agree with it; otherwise the
+//     CSR kernel at a width chosen without timing.
 #include <map>
 #include <mutex>
 
@@ -61,6 +64,27 @@ int width_no_alloc(const deco_csr_s* A, bool f32) {
   return sw ? sw : heuristic_subwarp(A->avg_row, f32 ? 4 : 2);
 }
 
+// One factor product with the kernel deco_fsai_apply would pick when that needs no
+// allocation: the slot-padded copies (scalar rows, or 2x2 cell blocks with x
+// aligned for pair loads), else the CSR kernel at the width chosen above.
+template <typename VT, typename XT, class Epi>
+void product_no_alloc(deco_ctx_s* ctx, deco_csr_s* A, const XT* x, Epi epi) {
+  const bool f32 = sizeof(VT) == 4;
+  if (A->ew && (!f32 || A->ev32)) {
+    if (!A->bbs) {
+      launch_ell1<VT, XT, Epi>(ctx->stream, A, x, epi);
+      return;
+    }
+    if (A->bbs == 2 && reinterpret_cast<uintptr_t>(x) % (2 * sizeof(XT)) == 0) {
+      launch_ell2<VT, XT, Epi>(ctx->stream, A, false, x, epi);
+      return;
+    }
+  }
+  const VT* v;
+  if constexpr (sizeof(VT) == 4) v = A->v32.get(); else v = A->v.get();
+  launch_spmv_sw<VT, XT>(ctx->stream, width_no_alloc(A, f32), A->n, 1, A->r.get(), A->c.get(), v, x, epi);
+}
+
 }  // namespace
 }  // namespace deco
 
@@ -73,19 +97,14 @@ extern "C" int deco_fsai_apply_static(deco_ctx ctx, deco_fsai F, const double* x
                  "deco_fsai_apply_static: the factor has more rows than the static scratch holds (" +
                      std::to_string(F->n) + " > " + std::to_string(kStaticRows) + "); use deco_fsai_apply");
     void* tmp = scratch_address(ctx->device);
-    const int n = F->n;
     if (F->precision == 32) {
       float* t = static_cast<float*>(tmp);
-      launch_spmv_sw<float, double>(ctx->stream, width_no_alloc(&F->FL, true), n, 1, F->FL.r.get(), F->FL.c.get(),
-                                    F->FL.v32.get(), x, EpiStore<float>{t});
-      launch_spmv_sw<float, float>(ctx->stream, width_no_alloc(&F->FUt, true), n, 1, F->FUt.r.get(), F->FUt.c.get(),
-                                   F->FUt.v32.get(), t, EpiStore<double>{y});
+      product_no_alloc<float, double>(ctx, &F->FL, x, EpiStore<float>{t});
+      product_no_alloc<float, float>(ctx, &F->FUt, t, EpiStore<double>{y});
     } else {
       double* t = static_cast<double*>(tmp);
-      launch_spmv_sw<double, double>(ctx->stream, width_no_alloc(&F->FL, false), n, 1, F->FL.r.get(), F->FL.c.get(),
-                                     F->FL.v.get(), x, EpiStore<double>{t});
-      launch_spmv_sw<double, double>(ctx->stream, width_no_alloc(&F->FUt, false), n, 1, F->FUt.r.get(),
-                                     F->FUt.c.get(), F->FUt.v.get(), t, EpiStore<double>{y});
+      product_no_alloc<double, double>(ctx, &F->FL, x, EpiStore<double>{t});
+      product_no_alloc<double, double>(ctx, &F->FUt, t, EpiStore<double>{y});
     }
   });
 }

@@ -42,6 +42,8 @@ struct deco_csr_s {
   deco::DevBuf<float> bv32;
   int bsw64 = 0, bsw32 = 0;
   double avg_blk = 0;
+  // Slot-padded copy (bbs == 2: of the cell blocks; bbs == 0: of the scalar rows,
+  // ec[k * n + i] / ev[k * n + i] holding row i's entry k).
   // Slot-padded copy of a 2x2-block matrix whose cells have at most `ew` blocks
   // (ew = 4 or 8; 0: none): every cell gets ew block slots, slot-major (slot k of
   // all cells contiguous), unused slots repeating one of the cell's columns (or
@@ -402,6 +404,49 @@ __global__ void __launch_bounds__(256) ell2_kernel(int nbr, const int* __restric
   }
 }
 
+// Slot-padded scalar product (a CSR matrix with at most W entries per row: the
+// FSAI factors of a pressure system): one thread per row, slot-major coalesced
+// loads.  Float32 values times float32 x: each group of four slots is summed in
+// float32 and converted once, as the CSR kernel sums one 128-bit value load.
+template <int W, typename VT, typename XT, class Epi>
+__global__ void __launch_bounds__(256) ell1_kernel(int n, const int* __restrict__ ec, const VT* __restrict__ ev,
+                                                   const XT* __restrict__ x, Epi epi) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int cc[W];
+  VT vv[W];
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    cc[k] = __ldcs(ec + (long long)k * n + i);
+    vv[k] = __ldcs(ev + (long long)k * n + i);
+  }
+  double sum = 0.0;
+  if constexpr (kRunF32<VT, XT>) {
+#pragma unroll
+    for (int g = 0; g < W; g += 4) {
+      float run = 0.f;
+#pragma unroll
+      for (int k = g; k < g + 4; ++k) run = fmaf(vv[k], __ldg(x + cc[k]), run);
+      sum += (double)run;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < W; ++k) sum += (double)vv[k] * (double)__ldg(x + cc[k]);
+  }
+  epi(i, sum);
+}
+
+template <typename VT, typename XT, class Epi>
+void launch_ell1(cudaStream_t st, const deco_csr_s* A, const XT* x, Epi epi) {
+  if (A->n <= 0) return;
+  const VT* ev;
+  if constexpr (sizeof(VT) == 4) ev = A->ev32.get(); else ev = A->ev.get();
+  const unsigned grid = (unsigned)cdiv(A->n, 256);
+  if (A->ew == 4) ell1_kernel<4, VT, XT, Epi><<<grid, 256, 0, st>>>(A->n, A->ec.get(), ev, x, epi);
+  else ell1_kernel<8, VT, XT, Epi><<<grid, 256, 0, st>>>(A->n, A->ec.get(), ev, x, epi);
+  DECO_CHECK_LAUNCH();
+}
+
 template <typename VT, typename XT, class Epi>
 void launch_ell2(cudaStream_t st, const deco_csr_s* A, bool row0, const XT* x, Epi epi) {
   const int nbr = A->n / 2;
@@ -489,6 +534,10 @@ void make_bsr(deco_ctx_s* ctx, deco_csr_s* A, int bs, double max_fill = 1.25);
 // 25 %; otherwise none), float32 values too when the block copy has them.
 // make_bsr and make_f32_values call it.
 void make_padded(deco_ctx_s* ctx, deco_csr_s* A);
+// The scalar slot-padded copy of a CSR matrix without cell blocks (4 slots when no
+// row has more than 4 entries, 8 when none has more than 8 and the padding stays
+// within 25 %), float32 values too when A has them; make_f32_values refreshes it.
+void make_padded_scalar(deco_ctx_s* ctx, deco_csr_s* A);
 void drop_bsr(deco_csr_s* A);
 
 // y = op(A x) over rows 0, bs, 2bs, ... (nrows_out = n / bs rows).  Uses the
@@ -504,6 +553,10 @@ void spmv(deco_ctx_s* ctx, deco_csr_s* A, const XT* x, Epi epi, int bs = 1) {
       return;
     }
     launch_bsr<VT, XT, Epi>(ctx->stream, A, tuned_bsr_subwarp(ctx, A, f32), bs != 1, x, epi);
+    return;
+  }
+  if (!A->bbs && A->ew && bs == 1 && (!f32 || A->ev32)) {
+    launch_ell1<VT, XT, Epi>(ctx->stream, A, x, epi);
     return;
   }
   const int sw = tuned_subwarp(ctx, A, f32);

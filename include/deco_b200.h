@@ -98,10 +98,11 @@ int deco_csr_set_subwarp(deco_csr A, int sw);
 int deco_csr_set_blocks(deco_ctx ctx, deco_csr A, int bs);
 int deco_csr_blocks(deco_csr A, int* bs, int* nblk);
 /* Slots per cell of the padded copy that products of a 2x2-block matrix use
- * when every cell has at most 4 blocks (or at most 8 with at most 25 % padding):
- * 4, 8, or 0 without one.  It is made with the block copy; DECO_PADDED=0 in the
- * environment at context creation turns it off.  No counterpart in the
- * reference. */
+ * when every cell has at most 4 blocks (or at most 8 with at most 25 % padding),
+ * or slots per row of the scalar padded copy that an FSAI factor without cell
+ * blocks gets under the same rule: 4, 8, or 0 without one.  The block form is
+ * made with the block copy; DECO_PADDED=0 in the environment at context
+ * creation turns both off.  No counterpart in the reference. */
 int deco_csr_padded(deco_csr A, int* slots);
 
 /* y = A x (bs == 1), or the restricted product of alg::spmv with bs > 1:
@@ -128,9 +129,10 @@ int deco_fsai_info(deco_fsai F, int* n, int* nz, int* max_order);
 /* Cell-block copies of the two factors (deco_csr_set_blocks): block size (0
  * without) and stored blocks of FL and of FU^T. */
 int deco_fsai_blocks(deco_fsai F, int* bs, int* nblk_lower, int* nblk_upper);
-/* Padded slots per cell of FL's and FU^T's 2x2-block copies (deco_csr_padded):
- * 4 for the factors of 7-point systems with power 1, 0 without.  No counterpart
- * in the reference. */
+/* Padded slots of FL and FU^T (deco_csr_padded): per cell of their 2x2-block
+ * copies, or per row for factors without cell blocks (the pressure FSAI); 4 for
+ * power-1 factors of 7-point systems, 0 without.  No counterpart in the
+ * reference. */
 int deco_fsai_padded(deco_fsai F, int* slots_lower, int* slots_upper);
 /* FL (lower, diagonal last) and FU^T (upper) in the reference's layout. */
 int deco_fsai_download(deco_ctx ctx, deco_fsai F, int* h_Lr, int* h_Lc, double* h_Lv, int* h_Ur, int* h_Uc,

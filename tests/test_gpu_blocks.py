@@ -132,8 +132,10 @@ def test_cpr_builds_blocks_and_keeps_parity(d, precision):
     P = d.CPR(prec, A, b, precision)
     assert A.blocks[0] == 2
     assert P.fsai(0).n == s.n
-    # power-1 factors of a 7-point system: at most 4 blocks per cell -> 4 padded slots
+    # power-1 factors of a 7-point system: at most 4 blocks per cell (global FSAI)
+    # and 4 entries per row (pressure FSAI) -> 4 padded slots
     assert P.fsai(0).padded == (4, 4)
+    assert P.fsai(1).padded == (4, 4)
     O = port.Cpr(prec, s.r, s.c, s.v, s.b)
     rvec = np.random.default_rng(5).standard_normal(s.n)
     tol = 1e-12 if precision == 64 else 1e-5
