@@ -228,6 +228,60 @@ __global__ void __launch_bounds__(256, 3) ell2_mm_kernel(int nbr, const int* __r
     for (int k = 0; k < K; ++k) epi(ROW0 ? s : 2 * s + q, k, acc[q][k]);
 }
 
+// K-column product of a scalar matrix with a slot-padded copy (see ell1_kernel):
+// one thread per row holds the row's K sums; float32 values times float32 x sum
+// each group of four slots in float32 per column, as the single-vector kernel.
+template <int W, int K, typename VT, typename XT, class Epi>
+__global__ void __launch_bounds__(256, 3) ell1_mm_kernel(int n, const int* __restrict__ ec, const VT* __restrict__ ev,
+                                                         const XT* __restrict__ x, Epi epi, MMGate gate) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (gate.active && __ldg(gate.active + __ldg(gate.cell_sys + i / gate.div)) == 0) return;
+  double acc[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) acc[k] = 0.0;
+#pragma unroll
+  for (int g = 0; g < W; g += 4) {
+    if constexpr (kRunF32<VT, XT>) {
+      float run[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k) run[k] = 0.f;
+#pragma unroll
+      for (int j = g; j < g + 4; ++j) {
+        const long long o = (long long)__ldcs(ec + (long long)j * n + i) * K;
+        const float v = __ldcs(ev + (long long)j * n + i);
+        float xv[K];
+        load_k_f32<K>(x, o, xv);
+#pragma unroll
+        for (int k = 0; k < K; ++k) run[k] = fmaf(v, xv[k], run[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < K; ++k) acc[k] += (double)run[k];
+    } else {
+#pragma unroll
+      for (int j = g; j < g + 4; ++j) {
+        const long long o = (long long)__ldcs(ec + (long long)j * n + i) * K;
+        const double v = (double)__ldcs(ev + (long long)j * n + i);
+        double xv[K];
+        load_k<K, XT>(x, o, xv);
+#pragma unroll
+        for (int k = 0; k < K; ++k) acc[k] += v * xv[k];
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) epi(i, k, acc[k]);
+}
+
+template <int K, typename VT, typename XT, class Epi>
+void launch_ell1_mm(cudaStream_t st, const deco_csr_s* A, const VT* ev, const XT* x, Epi epi, MMGate gate) {
+  if (A->n <= 0) return;
+  const unsigned grid = (unsigned)cdiv(A->n, 256);
+  if (A->ew == 4) ell1_mm_kernel<4, K, VT, XT, Epi><<<grid, 256, 0, st>>>(A->n, A->ec.get(), ev, x, epi, gate);
+  else ell1_mm_kernel<8, K, VT, XT, Epi><<<grid, 256, 0, st>>>(A->n, A->ec.get(), ev, x, epi, gate);
+  DECO_CHECK_LAUNCH();
+}
+
 template <int K, typename VT, typename XT, class Epi>
 void launch_ell2_mm(cudaStream_t st, const deco_csr_s* A, const VT* ev, bool row0, const XT* x, Epi epi,
                     MMGate gate) {
@@ -306,11 +360,12 @@ void spmm(deco_ctx_s* ctx, const deco_csr_s* A, const XT* x, Epi epi, bool row0 
     else gate = MMGate{};
   }
   cudaStream_t st = ctx->stream;
-  if (M.bs == 2 && A->ew) {
+  if (A->ew && (M.bs == 2 || (M.bs == 1 && !A->bbs && !row0))) {
     const VT* ev;
     if constexpr (sizeof(VT) == 4) ev = A->ev32.get(); else ev = A->ev.get();
     if (ev) {
-      launch_ell2_mm<K, VT, XT, Epi>(st, A, ev, row0, x, epi, gate);
+      if (M.bs == 2) launch_ell2_mm<K, VT, XT, Epi>(st, A, ev, row0, x, epi, gate);
+      else launch_ell1_mm<K, VT, XT, Epi>(st, A, ev, x, epi, gate);
       return;
     }
   }
