@@ -545,10 +545,10 @@ def main():
     dom = kernels["spmv_A_f32"]
     roofline = {"bound": "hbm", "achieved": dom["gbs"], "peak": peak, "unit": "GB/s", "frac": dom["gbs"] / peak,
                 # DRAM read + write bytes per launch of this kernel from one ncu capture of this
-                # workload: the padded kernel 672.0 MB read + 8.9 MB written
-                # (profiles/ell2_f32_config3_full.md); the pair kernel 604.8 + 11.5 MB
+                # workload: the padded kernel with 7 slots 592.0 MB read + 7.2 MB written
+                # (profiles/ell2_f32_config3_full.md; with 8 slots 672.0 + 8.9 MB); the pair kernel 604.8 + 11.5 MB
                 # (profiles/bsr2_pair_f32_config3_full.md)
-                "traffic": (680.9e6 if A.padded == 8 else 616.3e6 if A.blocks[0] == 2 and not A.padded else None),
+                "traffic": ({7: 599.2e6, 8: 680.9e6}.get(A.padded) if A.padded else 616.3e6 if A.blocks[0] == 2 else None),
                 "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/"
                                    + ("ell2_f32_config3_full.md" if A.padded else "bsr2_pair_f32_config3_full.md"))
                 if A.blocks[0] == 2 else None,

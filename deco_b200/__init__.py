@@ -196,7 +196,7 @@ class CSR:
 
     @property
     def padded(self):
-        """Slots per cell of the padded 2x2-block copy the products use (4 or 8; 0: none)."""
+        """Slots per cell (or row) of the padded copy the products use (4, 7 or 8; 0: none)."""
         w = C.c_int()
         check(lib().deco_csr_padded(self.h, C.byref(w)))
         return w.value
@@ -275,7 +275,7 @@ class FSAI:
 
     @property
     def padded(self):
-        """(slots of FL's, slots of FU^T's) padded 2x2-block copies: 4 or 8, 0 without."""
+        """(slots of FL's, slots of FU^T's) padded copies (4, 7 or 8; 0 without)."""
         a, b = C.c_int(), C.c_int()
         check(lib().deco_fsai_padded(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value

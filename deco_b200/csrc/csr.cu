@@ -102,7 +102,8 @@ void make_padded(deco_ctx_s* ctx, deco_csr_s* A) {
     DECO_CUDA(cudaStreamSynchronize(st));
     int W = 0;
     if (maxb <= 4) W = 4;
-    else if (maxb <= 8 && 8.0 * nbr <= 1.25 * A->nblk) W = 8;
+    else if (maxb <= 8) W = maxb <= 7 ? 7 : 8;  // 7: the widest cell of a 7-point system, no padding
+    if (W > 4 && (double)W * nbr > 1.25 * A->nblk) W = 0;
     if (!W) return;
     A->ew = W;
     A->ec.alloc((size_t)W * nbr, st);

@@ -291,6 +291,9 @@ void launch_ell2_mm(cudaStream_t st, const deco_csr_s* A, const VT* ev, bool row
   if (A->ew == 4) {
     if (row0) ell2_mm_kernel<4, K, true, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, gate);
     else ell2_mm_kernel<4, K, false, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, gate);
+  } else if (A->ew == 7) {
+    if (row0) ell2_mm_kernel<7, K, true, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, gate);
+    else ell2_mm_kernel<7, K, false, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, gate);
   } else {
     if (row0) ell2_mm_kernel<8, K, true, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, gate);
     else ell2_mm_kernel<8, K, false, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, gate);

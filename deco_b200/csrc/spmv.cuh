@@ -45,7 +45,7 @@ struct deco_csr_s {
   // Slot-padded copy (bbs == 2: of the cell blocks; bbs == 0: of the scalar rows,
   // ec[k * n + i] / ev[k * n + i] holding row i's entry k).
   // Slot-padded copy of a 2x2-block matrix whose cells have at most `ew` blocks
-  // (ew = 4 or 8; 0: none): every cell gets ew block slots, slot-major (slot k of
+  // (ew = 4, 7 or 8 for cell blocks, 4 or 8 for scalar rows; 0: none): every cell gets ew block slots, slot-major (slot k of
   // all cells contiguous), unused slots repeating one of the cell's columns (or
   // column 0) with zero values.  ec[k * ncell + s]: block column; value plane q (in-block row q),
   // slot k: the block row's two values at pair index (q * ew + k) * ncell + s.
@@ -457,6 +457,9 @@ void launch_ell2(cudaStream_t st, const deco_csr_s* A, bool row0, const XT* x, E
   if (A->ew == 4) {
     if (row0) ell2_kernel<4, true, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi);
     else ell2_kernel<4, false, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi);
+  } else if (A->ew == 7) {
+    if (row0) ell2_kernel<7, true, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi);
+    else ell2_kernel<7, false, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi);
   } else {
     if (row0) ell2_kernel<8, true, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi);
     else ell2_kernel<8, false, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi);
@@ -530,8 +533,9 @@ int tuned_bsr_subwarp(deco_ctx_s* ctx, deco_csr_s* A, bool f32);
 // block copy.  Float32 planes are made when A has float32 values.
 void make_bsr(deco_ctx_s* ctx, deco_csr_s* A, int bs, double max_fill = 1.25);
 // Builds the slot-padded copy of a 2x2-block matrix (4 slots when no cell has
-// more than 4 blocks, 8 when none has more than 8 and the padding stays within
-// 25 %; otherwise none), float32 values too when the block copy has them.
+// more than 4 blocks, else 7 or 8, the fewest that hold the widest cell, when the
+// padding stays within 25 %; otherwise none), float32 values too when the block
+// copy has them.
 // make_bsr and make_f32_values call it.
 void make_padded(deco_ctx_s* ctx, deco_csr_s* A);
 // The scalar slot-padded copy of a CSR matrix without cell blocks (4 slots when no

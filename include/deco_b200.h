@@ -98,9 +98,10 @@ int deco_csr_set_subwarp(deco_csr A, int sw);
 int deco_csr_set_blocks(deco_ctx ctx, deco_csr A, int bs);
 int deco_csr_blocks(deco_csr A, int* bs, int* nblk);
 /* Slots per cell of the padded copy that products of a 2x2-block matrix use
- * when every cell has at most 4 blocks (or at most 8 with at most 25 % padding),
- * or slots per row of the scalar padded copy that an FSAI factor without cell
- * blocks gets under the same rule: 4, 8, or 0 without one.  The block form is
+ * when every cell has at most 4 blocks (4 slots) or at most 7 or 8 blocks with
+ * at most 25 % padding (7 or 8 slots), or slots per row of the scalar padded
+ * copy that an FSAI factor without cell blocks gets (4, or 8 with at most 25 %
+ * padding); 0 without one.  The block form is
  * made with the block copy; DECO_PADDED=0 in the environment at context
  * creation turns both off.  No counterpart in the reference. */
 int deco_csr_padded(deco_csr A, int* slots);

@@ -44,8 +44,8 @@ def test_block_products_match_oracle(d, name):
     A.set_blocks(s.bs)
     bs, nblk = A.blocks
     assert bs == s.bs and nblk * bs * bs == s.nnz  # generated systems are dense cell blocks
-    # 7-point cells carry up to 7 blocks: 8 padded slots when that pads at most 25 %
-    assert A.padded == (8 if bs == 2 and 8 * (s.n // 2) <= 1.25 * nblk else 0)
+    # 7-point cells carry up to 7 blocks: 7 padded slots when that pads at most 25 %
+    assert A.padded == (7 if bs == 2 and 7 * (s.n // 2) <= 1.25 * nblk else 0)
     x = np.random.default_rng(0).standard_normal(s.n)
     assert rel(A.apply(cuda(x)).cpu().numpy(), port.spmv(s.r, s.c, s.v, x)) < 1e-12
     assert rel(A.apply(cuda(x), bs=s.bs).cpu().numpy(), port.spmv(s.r, s.c, s.v, x, s.bs)) < 1e-12
