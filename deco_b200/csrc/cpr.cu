@@ -89,8 +89,20 @@ __device__ void small_lu_solve(int k, double* M, double* b) {
   }
 }
 
+// Per-cell scratch arrays are written at positions that come from the data
+// (column % bs); store_at spells such a write as an unrolled compare-and-select
+// so that, with the block size a template constant, every array stays in
+// registers (with a run-time bs they spilled to a 432-byte stack frame).
+template <int N>
+__device__ __forceinline__ void store_at(double* arr, int idx, double val) {
+#pragma unroll
+  for (int t = 0; t < N; ++t)
+    if (t == idx) arr[t] = val;
+}
+
+template <int BS>  // 2 or 3; 0: the block size from a.bs (at most 3)
 __global__ void cpr_decouple(DecoupleArgs a) {
-  const int bs = a.bs;
+  const int bs = BS > 0 ? BS : a.bs;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.sn; s += gridDim.x * blockDim.x) {
     const int* __restrict__ r = a.r;
     const int* __restrict__ c = a.c;
@@ -137,7 +149,7 @@ __global__ void cpr_decouple(DecoupleArgs a) {
         const int j = bsearch_le(c, r[i], r[i + 1], i);
         for (int k = 1; k < bs; ++k) {
           if (p == 0) bp[k - 1] = -v[j + k - p];
-          else Apb[(p - 1) * (bs - 1) + c[j + k - p] % bs - 1] = v[j + k - p];
+          else store_at<4>(Apb, (p - 1) * (bs - 1) + c[j + k - p] % bs - 1, v[j + k - p]);
         }
       }
       if (bs == 3) {
@@ -164,7 +176,7 @@ __global__ void cpr_decouple(DecoupleArgs a) {
         for (int k = 0; k < bs; ++k) {
           const int q = j + k - p;
           if (q < ia || q >= ib) continue;
-          if (c[q] / bs == s) B[p * bs + c[q] % bs] = v[q];
+          if (c[q] / bs == s) store_at<9>(B, p * bs + c[q] % bs, v[q]);
         }
       }
       w[0] = 0.0; w[1] = 0.0; w[2] = 0.0;
@@ -198,7 +210,9 @@ __global__ void cpr_decouple(DecoupleArgs a) {
         for (int j = ia; j < ib; ++j) {
           if (j == jd) continue;
           const int q = c[j] % bs;
-          off[q] = dadd(off[q], fabs(v[j]));
+#pragma unroll
+          for (int t = 0; t < 3; ++t)
+            if (t == q) off[t] = dadd(off[t], fabs(v[j]));
         }
         for (int p = 0; p < bs; ++p) wd[p] = wd[p] && !(off[p] < dmul(a.e_ps, diag));
       }
@@ -246,7 +260,7 @@ __global__ void cpr_decouple(DecoupleArgs a) {
         const int i = i0 + p;
         const int j = bsearch_le(c, r[i], r[i + 1], i);
         Dp[p] = v[j];
-        for (int k = 0; k < bs; ++k) B[p * bs + c[j + k - p] % bs] = v[j + k - p];
+        for (int k = 0; k < bs; ++k) store_at<9>(B, p * bs + c[j + k - p] % bs, v[j + k - p]);
       }
       if (bs == 3) {
         const double c0 = dsub(dmul(B[4], B[8]), dmul(B[5], B[7]));
@@ -487,7 +501,9 @@ static void cpr_build(deco_ctx_s* ctx, deco_csr_s* A, double* d_b, const deco_cp
   a.e_dd = prm.drs_e_dd; a.e_ps = prm.drs_e_ps;
   a.r = A->r.get(); a.c = A->c.get(); a.v = A->v.get(); a.b = d_b;
   a.w = P->w.get(); a.w0 = P->w0.get(); a.ops = P->ops.get(); a.J = P->J.get(); a.chk = P->check_diag.get(); a.err = flags.get(); a.nfixed = flags.get() + 1;
-  cpr_decouple<<<grid_for(ctx, P->sn, 128, 16), 128, 0, st>>>(a);
+  if (bs == 2) cpr_decouple<2><<<grid_for(ctx, P->sn, 128, 16), 128, 0, st>>>(a);
+  else if (bs == 3) cpr_decouple<3><<<grid_for(ctx, P->sn, 128, 16), 128, 0, st>>>(a);
+  else cpr_decouple<0><<<grid_for(ctx, P->sn, 128, 16), 128, 0, st>>>(a);
   DECO_CHECK_LAUNCH();
   int hf[2];
   DECO_CUDA(cudaMemcpyAsync(hf, flags.get(), sizeof(hf), cudaMemcpyDeviceToHost, st));
