@@ -97,7 +97,8 @@ __device__ __forceinline__ bool last_block(unsigned* counter) {
   __shared__ bool amlast;
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) amlast = atomicInc(counter, gridDim.x - 1) == gridDim.x - 1;
+  const unsigned nblk = gridDim.x * gridDim.y;  // the ticket wraps to 0 for the next launch
+  if (threadIdx.x == 0) amlast = atomicInc(counter, nblk - 1) == nblk - 1;
   __syncthreads();
   return amlast;
 }
@@ -196,7 +197,9 @@ __device__ __forceinline__ double vdot(const float4& a, const float4& b) {
 // the tiles of w and u_j are copied into shared memory (double-buffered cp.async,
 // so the next tile streams in while this one is used) and warp w streams columns
 // w, w+8, ... (CPW of them: the template is the smallest power of two with
-// 8*CPW >= ncols) against them, keeping per-column partial sums in registers.
+// 8*CPW >= ncols, at most 4; past 32 columns a second block per row range,
+// blockIdx.y = 1, takes columns 32..63) against them, keeping per-column
+// partial sums in registers.
 // Rows past the last full vector are summed by the last block.  (Measured on
 // B200, float32 basis, 8M rows, 26 columns: 168 us against 370 us when every
 // warp held w and u_j in registers and formed each product in float64; the
@@ -213,6 +216,7 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long 
   __shared__ __align__(16) VT ws[2][kTileVec];
   __shared__ __align__(16) VT us[2][kTileVec];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int cbase = blockIdx.y * (kWarps * CPW);  // a second block row of the grid takes the next columns
   const long long nvec = n / N;
   const long long per = (nvec + gridDim.x - 1) / gridDim.x;
   const long long v0 = min(nvec, per * blockIdx.x), v1 = min(nvec, v0 + per);
@@ -249,7 +253,7 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long 
     const long long t0 = v0 + (long long)t * kTileVec;
 #pragma unroll
     for (int k = 0; k < CPW; ++k) {
-      const int c = warp + k * kWarps;
+      const int c = cbase + warp + k * kWarps;
       if (c < ncols) {
         const VT* __restrict__ vc = reinterpret_cast<const VT*>(V + (size_t)c * ld);
         for (int s0 = 0; s0 < kTileVec; s0 += 32 * kVecPerLane) {
@@ -275,7 +279,7 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long 
     for (long long r = nvec * N; r < n; ++r)
 #pragma unroll
       for (int k = 0; k < CPW; ++k) {
-        const int c = warp + k * kWarps;
+        const int c = cbase + warp + k * kWarps;
         if (c < ncols) {
           const double v = (double)V[(size_t)c * ld + r];
           pw[k] += v * (double)w[r];
@@ -285,7 +289,7 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long 
   }
 #pragma unroll
   for (int k = 0; k < CPW; ++k) {
-    const int c = warp + k * kWarps;
+    const int c = cbase + warp + k * kWarps;
     const double a = warp_sum(pw[k]), b = warp_sum(pu[k]);
     if (lane == 0 && c < ncols) {
       red[(size_t)c * gridDim.x + blockIdx.x] = a;
@@ -381,8 +385,10 @@ void launch_arnoldi_dots(cudaStream_t s, int nb, long long n, long long ld, int 
     arnoldi_dots<T, 2><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V, w, red, counter, st);
   else if (nc <= 4 * kWarps)
     arnoldi_dots<T, 4><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V, w, red, counter, st);
-  else
-    arnoldi_dots<T, 8><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V, w, red, counter, st);
+  else  // two blocks per row range, 32 columns each: 56 registers instead of 76 for 8 columns per warp, at the
+        // cost of reading the w and u_j tiles twice (measured on the 8M-row system at restart 50: the
+        // orthogonalisation 0.343 against 0.353 ms per iteration)
+    arnoldi_dots<T, 4><<<dim3(nb, 2), kThreads, 0, s>>>(n, ld, nc, j, V, w, red, counter, st);
 }
 
 // ---- pass B: w'' = w - sum_c coef_c u_c, stored as column j+1; ||w''||^2.
