@@ -48,7 +48,7 @@ os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
 METRIC = "CPR-GMRES time-to-1e-8 (mixed vs FP64, same B200); SpMV/FSAI HBM GB/s"
 CONFIG = 3
 SEED = 1234
-WORKLOAD = ("config 3: 200x200x100 two-phase grid, bs=2, 8,000,000 rows, 111,360,000 nnz, lognormal k sigma 2.5 "
+WORKLOAD = ("200x200x100 two-phase grid, bs=2, 8,000,000 rows, 111,360,000 nnz, lognormal k sigma 2.5 "
             "+ 1e4-contrast channels; CPR(FSAI global p1 + FSAI pressure p1, seq 3, quasiimpes_GE, CPD) "
             "+ right GMRES(50), true relative residual 1e-8")
 PREC = {"type": "CPR", "block_size": "2", "pressure_id": "0", "seq": "3", "weights": "quasiimpes_GE",
@@ -215,7 +215,7 @@ def bench_batch(args):
             "value": out["mixed"]["time_s"], "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": False, "scaling": "strong", "dtype": "f32+f64",
             "data": "synthetic",
-            "config": {"workload": f"config 4: 64 two-phase systems, cells log-uniform 10k-500k ({n_all // 2} cells, "
+            "config": {"workload": f"64 two-phase systems, cells log-uniform 10k-500k ({n_all // 2} cells, "
                                    f"{n_all} rows, {nnz_all} nnz), 8 uniform right-hand sides each; CPR seq 3 + "
                                    f"GMRES(50)", "seed": SEED,
                        "parallelism": f"systems dealt round-robin to {world} GPU(s), no collective"}, **out,
@@ -337,7 +337,7 @@ def bench_adjoint(args):
                       "value": (out["fp64"]["forward_ms"] + out["fp64"]["adjoint_ms"] + out["fp64"]["grad_kernel_ms"])
                       / 1e3, "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
                       "higher_is_better": False, "dtype": "f64", "data": "synthetic",
-                      "config": {"workload": "config 5: 64x64x32 two-phase grid from a seeded log-permeability "
+                      "config": {"workload": "64x64x32 two-phase grid from a seeded log-permeability "
                                              "field, bs 2, 262,144 rows; L = weighted pressures at 20 seeded cells; "
                                              "CPR seq 3 + GMRES(50) to 1e-8 forward and adjoint", "seed": SEED},
                       **out}))
@@ -354,9 +354,10 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only the per-kernel timings (for profiler captures on a smaller --config)")
-    ap.add_argument("--config", type=int, default=3, help="system preset (3 = the benchmark workload)")
+    ap.add_argument("--config", type=int, default=3, help="system preset (3 = the 200x200x100 benchmark workload)")
     ap.add_argument("--workload", default="solve", choices=["solve", "batch", "adjoint", "spmv"],
-                    help="solve: the headline single-system solve; batch: config 4; adjoint: config 5; "
+                    help="solve: the headline single-system solve; batch: 64 systems x 8 right-hand sides; "
+                         "adjoint: the 64x64x32 log-permeability gradient; "
                          "spmv: the SpMV kernels alone")
     args = ap.parse_args()
     if args.workload == "batch":

@@ -133,7 +133,7 @@ def uniform(seed: int, stream: int, n: int) -> np.ndarray:
 
 
 def grid(nx: int, ny: int, nz: int, bs: int = 2, seed: int = 1234, **kw) -> System:
-    """Small custom grid with the config-1 value distributions (for tests)."""
+    """Small custom grid with the value distributions of preset 1 (for tests)."""
     p = preset(1, seed)
     p.nx, p.ny, p.nz, p.bs = nx, ny, nz, bs
     for k, val in kw.items():
@@ -143,7 +143,7 @@ def grid(nx: int, ny: int, nz: int, bs: int = 2, seed: int = 1234, **kw) -> Syst
 
 def batch(nsys: int = 64, seed: int = 1234, cells_lo: int = 10_000, cells_hi: int = 500_000, bs: int = 2,
           nrhs: int = 8):
-    """Independent two-phase systems (the config-1 value distributions) with cell
+    """Independent two-phase systems (the value distributions of preset 1) with cell
     counts drawn log-uniform in [cells_lo, cells_hi], concatenated into one
     block-diagonal CSR, plus `nrhs` uniform [0,1) right-hand sides per system
     (row-interleaved).  Returns (r, c, v, row_off, B, shapes)."""
