@@ -13,17 +13,74 @@
 
 namespace deco {
 
+// K values of one multi-vector row from / to doubles with 16-byte accesses
+// (scalar ones when K does not fill them)
+template <int K, typename T>
+__device__ __forceinline__ void row_load(const T* __restrict__ p, double* v) {
+  if (reinterpret_cast<uintptr_t>(p) % 16 != 0) {  // a caller's vector that is not 16-byte aligned
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = (double)p[k];
+    return;
+  }
+  if constexpr (sizeof(T) == 4 && K % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < K / 4; ++q) {
+      const float4 t = reinterpret_cast<const float4*>(p)[q];
+      v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
+    }
+  } else if constexpr (sizeof(T) == 8 && K % 2 == 0) {
+#pragma unroll
+    for (int q = 0; q < K / 2; ++q) {
+      const double2 t = reinterpret_cast<const double2*>(p)[q];
+      v[2 * q] = t.x; v[2 * q + 1] = t.y;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = (double)p[k];
+  }
+}
+template <int K, typename T>
+__device__ __forceinline__ void row_store(T* p, const double* v) {
+  if (reinterpret_cast<uintptr_t>(p) % 16 != 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) p[k] = (T)v[k];
+    return;
+  }
+  if constexpr (sizeof(T) == 4 && K % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < K / 4; ++q)
+      reinterpret_cast<float4*>(p)[q] =
+          make_float4((float)v[4 * q], (float)v[4 * q + 1], (float)v[4 * q + 2], (float)v[4 * q + 3]);
+  } else if constexpr (sizeof(T) == 8 && K % 2 == 0) {
+#pragma unroll
+    for (int q = 0; q < K / 2; ++q) reinterpret_cast<double2*>(p)[q] = make_double2(v[2 * q], v[2 * q + 1]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < K; ++k) p[k] = (T)v[k];
+  }
+}
+
 // ------------------------------------------------------------ epilogues
+// epi.row(row, v): all K values of one output row at once (16-byte accesses;
+// the same per-element arithmetic as epi(row, k, v[k]))
 // epi(row, k, value): value = (A X)[row][k] (row = cell for a restricted product)
 template <int K, typename YT> struct MStore {
   YT* y;
   __device__ void operator()(int row, int k, double v) const { y[(long long)row * K + k] = (YT)v; }
+  __device__ void row(int row, const double* v) const { row_store<K>(y + (long long)row * K, v); }
 };
 template <int K, typename YT> struct MAdd {
   YT* y;
   __device__ void operator()(int row, int k, double v) const {
     const long long o = (long long)row * K + k;
     y[o] = (YT)((double)y[o] + v);
+  }
+  __device__ void row(int row, const double* v) const {
+    double o[K];
+    row_load<K>(y + (long long)row * K, o);
+#pragma unroll
+    for (int k = 0; k < K; ++k) o[k] = o[k] + v[k];
+    row_store<K>(y + (long long)row * K, o);
   }
 };
 template <int K, typename ZT, typename YT> struct MResid {  // y = z - A x
@@ -32,11 +89,25 @@ template <int K, typename ZT, typename YT> struct MResid {  // y = z - A x
     const long long o = (long long)row * K + k;
     y[o] = (YT)((double)z[o] - v);
   }
+  __device__ void row(int row, const double* v) const {
+    double o[K];
+    row_load<K>(z + (long long)row * K, o);
+#pragma unroll
+    for (int k = 0; k < K; ++k) o[k] = o[k] - v[k];
+    row_store<K>(y + (long long)row * K, o);
+  }
 };
 template <int K, typename ZT, typename YT> struct MRestrict {  // y[s] = r[s*bs+p] - (A x)[s*bs]
   const ZT* r; YT* y; int bs, p;
   __device__ void operator()(int s, int k, double v) const {
     y[(long long)s * K + k] = (YT)((double)r[((long long)s * bs + p) * K + k] - v);
+  }
+  __device__ void row(int s, const double* v) const {
+    double o[K];
+    row_load<K>(r + ((long long)s * bs + p) * K, o);
+#pragma unroll
+    for (int k = 0; k < K; ++k) o[k] = o[k] - v[k];
+    row_store<K>(y + (long long)s * K, o);
   }
 };
 template <int K, typename YT> struct MProlong {  // x[s*bs+p] += (F t)[s]
@@ -44,6 +115,14 @@ template <int K, typename YT> struct MProlong {  // x[s*bs+p] += (F t)[s]
   __device__ void operator()(int s, int k, double v) const {
     const long long o = ((long long)s * bs + p) * K + k;
     x[o] = (YT)((double)x[o] + v);
+  }
+  __device__ void row(int s, const double* v) const {
+    YT* px = x + ((long long)s * bs + p) * K;
+    double o[K];
+    row_load<K>(px, o);
+#pragma unroll
+    for (int k = 0; k < K; ++k) o[k] = o[k] + v[k];
+    row_store<K>(px, o);
   }
 };
 // y = scale[q] * (A x) with q = system(row) * K + k: the per-instance scale of the
@@ -54,6 +133,13 @@ template <int K, typename YT> struct MStoreScaled {
   __device__ void operator()(int row, int k, double v) const {
     const int sys = __ldg(cell_sys + row / bs);
     y[(long long)row * K + k] = (YT)(__ldg(scale + (long long)(sys * K + k) * stride) * v);
+  }
+  __device__ void row(int row, const double* v) const {
+    const int sys = __ldg(cell_sys + row / bs);
+    double o[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) o[k] = __ldg(scale + (long long)(sys * K + k) * stride) * v[k];
+    row_store<K>(y + (long long)row * K, o);
   }
 };
 
@@ -223,9 +309,7 @@ __global__ void __launch_bounds__(256, 3) ell2_mm_kernel(int nbr, const int* __r
     }
   }
 #pragma unroll
-  for (int q = 0; q < NR; ++q)
-#pragma unroll
-    for (int k = 0; k < K; ++k) epi(ROW0 ? s : 2 * s + q, k, acc[q][k]);
+  for (int q = 0; q < NR; ++q) epi.row(ROW0 ? s : 2 * s + q, acc[q]);
 }
 
 // K-column product of a scalar matrix with a slot-padded copy (see ell1_kernel):
@@ -269,8 +353,7 @@ __global__ void __launch_bounds__(256, 3) ell1_mm_kernel(int n, const int* __res
       }
     }
   }
-#pragma unroll
-  for (int k = 0; k < K; ++k) epi(i, k, acc[k]);
+  epi.row(i, acc);
 }
 
 template <int K, typename VT, typename XT, class Epi>
