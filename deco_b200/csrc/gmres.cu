@@ -520,12 +520,41 @@ __global__ void backsolve(State st, int j) {
 
 // out = sum_{i < ncols} c_i u_i  (rgmres.tpp:106-109: w = g_0 v_0, then w += g_i v_i)
 template <typename T, typename Y>
-__global__ void combine(long long n, long long ld, int ncols, const T* __restrict__ V, const double* __restrict__ c,
-                        Y* __restrict__ out) {
-  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
-    double s = c[0] * (double)V[r];
-    for (int i = 1; i < ncols; ++i) s += c[i] * (double)V[(size_t)i * ld + r];
-    out[r] = (Y)s;
+__global__ void __launch_bounds__(kThreads) combine(long long n, long long ld, int ncols, const T* __restrict__ V,
+                                                    const double* __restrict__ c, Y* __restrict__ out) {
+  // one thread per 128-bit vector of rows, coefficients in shared memory, the
+  // column loop unrolled so several vector loads are in flight (each element
+  // sums in the same order as a row-by-row loop)
+  using VT = typename Vec4<T>::t;
+  constexpr int N = Vec4<T>::N;
+  __shared__ double cs[kMaxCols];
+  for (int i = threadIdx.x; i < ncols; i += kThreads) cs[i] = c[i];
+  __syncthreads();
+  const long long nvec = n / N;
+  for (long long vi = (long long)blockIdx.x * kThreads + threadIdx.x; vi < nvec;
+       vi += (long long)gridDim.x * kThreads) {
+    double s[N];
+    {
+      const VT v = __ldcs(reinterpret_cast<const VT*>(V) + vi);
+#pragma unroll
+      for (int e = 0; e < N; ++e) s[e] = cs[0] * Vec4<T>::get(v, e);
+    }
+#pragma unroll 4
+    for (int i = 1; i < ncols; ++i) {
+      const VT v = __ldcs(reinterpret_cast<const VT*>(V + (size_t)i * ld) + vi);
+      const double ci = cs[i];
+#pragma unroll
+      for (int e = 0; e < N; ++e) s[e] += ci * Vec4<T>::get(v, e);
+    }
+#pragma unroll
+    for (int e = 0; e < N; ++e) out[vi * N + e] = (Y)s[e];
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {  // rows past the last full vector
+    for (long long r = nvec * N; r < n; ++r) {
+      double s = cs[0] * (double)V[r];
+      for (int i = 1; i < ncols; ++i) s += cs[i] * (double)V[(size_t)i * ld + r];
+      out[r] = (Y)s;
+    }
   }
 }
 
