@@ -506,16 +506,34 @@ __global__ void __launch_bounds__(kThreads) norm2_kernel(long long n, const X* _
 
 // back substitution g(1:j) = H(1:j,1:j) \ g(1:j)  (rgmres.tpp:95-104), then the
 // coefficients on the stored columns c_i = y_i s_i
-__global__ void backsolve(State st, int j) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  st.sc[SC_BREAK] = 0.0;
+// One block: the upper triangle of H's first j columns and g are staged in
+// shared memory, then column by column g_i /= H(i,i) and, in parallel over k < i,
+// g_k -= H(k,i) g_i (every element sees the same operations in the same order as
+// the sequential column-oriented substitution).
+__global__ void __launch_bounds__(kThreads) backsolve(State st, int j) {
+  __shared__ double hs[(kMaxCols + 1) * kMaxCols];
+  __shared__ double g[kMaxCols + 1];
+  const int ldh = st.m + 1;
+  for (int i = 0; i < j; ++i)
+    for (int k = threadIdx.x; k <= i; k += kThreads) hs[k + i * ldh] = st.h(k, i);
+  for (int k = threadIdx.x; k <= j; k += kThreads) g[k] = st.g[k];
+  __syncthreads();
   for (int i = j - 1; i >= 0; --i) {
-    if (st.h(i, i) == 0.0) { st.sc[SC_BREAK] = 1.0; return; }
-    st.g[i] /= st.h(i, i);
-    for (int k = 0; k < i; ++k) st.g[k] -= st.h(k, i) * st.g[i];
+    const double hii = hs[i + i * ldh];
+    if (hii == 0.0) {  // the same value in every thread: the whole block leaves
+      if (threadIdx.x == 0) st.sc[SC_BREAK] = 1.0;
+      return;
+    }
+    if (threadIdx.x == 0) g[i] /= hii;
+    __syncthreads();
+    const double gi = g[i];
+    for (int k = threadIdx.x; k < i; k += kThreads) g[k] -= hs[k + i * ldh] * gi;
+    __syncthreads();
   }
+  if (threadIdx.x == 0) st.sc[SC_BREAK] = 0.0;
+  for (int k = threadIdx.x; k <= j; k += kThreads) st.g[k] = g[k];
   const int nc = j > 0 ? j : 1;
-  for (int i = 0; i < nc; ++i) st.c[i] = st.g[i] * st.s[i];
+  for (int i = threadIdx.x; i < nc; i += kThreads) st.c[i] = g[i] * st.s[i];
 }
 
 // out = sum_{i < ncols} c_i u_i  (rgmres.tpp:106-109: w = g_0 v_0, then w += g_i v_i)
@@ -758,7 +776,7 @@ struct Solver {
         ++j;
       }
       iter = base + j;
-      backsolve<<<1, 1, 0, s>>>(st, j);
+      backsolve<<<1, kThreads, 0, s>>>(st, j);
       DECO_CHECK_LAUNCH();
       DECO_CUDA(cudaMemcpyAsync(const_cast<double*>(hsc) + 3, st.sc + SC_BREAK, sizeof(double), cudaMemcpyDeviceToHost, s));
       DECO_CUDA(cudaStreamSynchronize(s));
