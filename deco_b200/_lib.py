@@ -47,6 +47,7 @@ SIGNATURES = {
     "deco_last_error": ([], C.c_char_p),
     "deco_version": ([], C.c_char_p),
     "deco_launch_count": ([], C.c_longlong),
+    "deco_alloc_count": ([], C.c_longlong),
     "deco_ctx_create": ([C.c_int, vp, C.POINTER(vp)], C.c_int),
     "deco_ctx_destroy": ([vp], C.c_int),
     "deco_ctx_sync": ([vp], C.c_int),

@@ -38,6 +38,10 @@ namespace {
 constexpr int kT = 256;            // threads per block of the batch kernels
 constexpr int kChunkRows = 4096;   // rows per dot chunk (chunks never cross systems)
 constexpr double kEpsB = 2.220446049250312e-16;
+// largest restart length: the kernels keep one coefficient per (basis column,
+// right-hand side) in dynamic shared memory, K (m + 1) doubles (32 KB at m = 512
+// and K = 8, under the 48 KB a block gets without opting in)
+constexpr int kMaxRestartB = 512;
 
 // per-instance state, `stride` doubles each: H (m+1)m | G (m+1)^2 | g | cs | sn | s | c | misc
 struct BState {
@@ -341,7 +345,7 @@ __global__ void __launch_bounds__(kT) b_update_v(const int* crow, const int* csy
                                                  T* __restrict__ out, double* __restrict__ red, int nchunk) {
   using S = VShape<K, T>;
   constexpr int E = S::E, P = S::P;
-  __shared__ double cf[64][K];
+  extern __shared__ double cf_u[];  // [nc][K] coefficients
   __shared__ double part[(kT / 32) * P * E];
   __shared__ double tot[P * E];
   const int c = blockIdx.x, sys = csys[c], nc = j + 1;
@@ -351,7 +355,7 @@ __global__ void __launch_bounds__(kT) b_update_v(const int* crow, const int* csy
   }
   for (int t = threadIdx.x; t < K * nc; t += kT) {
     const int i = t / K, kk = t % K, qi = sys * K + kk;
-    cf[i][kk] = in.active[qi] ? st.c(qi)[i] : 0.0;
+    cf_u[i * K + kk] = in.active[qi] ? st.c(qi)[i] : 0.0;
   }
   __syncthreads();
   const long long f0 = (long long)crow[c] * K / E, f1 = (long long)crow[c + 1] * K / E;
@@ -367,7 +371,7 @@ __global__ void __launch_bounds__(kT) b_update_v(const int* crow, const int* csy
       double v[E];
       vload<T, E>(V + (long long)i * ld + f * E, v, true);
 #pragma unroll
-      for (int q = 0; q < E; ++q) x[q] -= cf[i][E * ph + q] * v[q];
+      for (int q = 0; q < E; ++q) x[q] -= cf_u[i * K + E * ph + q] * v[q];
     }
     T o[E];
 #pragma unroll
@@ -382,11 +386,13 @@ __global__ void __launch_bounds__(kT) b_update_v(const int* crow, const int* csy
 }
 
 // one warp per instance: h, the Gram row of u_j, c = h + (h - G h), H(:,j), coefficients
+// (dynamic shared memory: (kT / 32) (j + 1) doubles, h of each warp's instance)
 template <int K>
 __global__ void b_dots_fin(int Q, const int* sch, BState st, Inst in, int j, const double* __restrict__ red,
                            int nchunk) {
-  __shared__ double hs[kT / 32][64];
+  extern __shared__ double hs_f[];
   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  double* hw = hs_f + (size_t)wl * (j + 1);
   const int qi = blockIdx.x * (kT / 32) + wl;
   if (qi >= Q || !in.active[qi]) return;
   const int sys = qi / K, k = qi % K, nc = j + 1;
@@ -398,7 +404,7 @@ __global__ void b_dots_fin(int Q, const int* sch, BState st, Inst in, int j, con
       a += red[((long long)i * K + k) * nchunk + c];
       b += red[((long long)(nc + i) * K + k) * nchunk + c];
     }
-    hs[wl][i] = a * s[i];
+    hw[i] = a * s[i];
     const double gij = s[i] * sj * b;
     st.G(qi, i, j) = gij;
     st.G(qi, j, i) = gij;
@@ -406,8 +412,8 @@ __global__ void b_dots_fin(int Q, const int* sch, BState st, Inst in, int j, con
   __syncwarp();
   for (int i = lane; i < nc; i += 32) {
     double gh = 0.0;
-    for (int t = 0; t < nc; ++t) gh += st.G(qi, i, t) * hs[wl][t];
-    const double ci = hs[wl][i] + (hs[wl][i] - gh);
+    for (int t = 0; t < nc; ++t) gh += st.G(qi, i, t) * hw[t];
+    const double ci = hw[i] + (hw[i] - gh);
     st.H(qi, i, j) = ci;
     st.c(qi)[i] = ci * s[i];
   }
@@ -490,12 +496,12 @@ __global__ void b_backsolve(int Q, BState st, Inst in, int* breakdown) {
 template <int K, typename T>
 __global__ void __launch_bounds__(kT) b_combine(const int* crow, const int* csys, BState st, long long ld, int ncols,
                                                 const T* __restrict__ V, double* __restrict__ out) {
-  __shared__ double cf[K][64];
+  extern __shared__ double cf_c[];  // [K][ncols] coefficients
   __shared__ int ncq[K];
   const int c = blockIdx.x, sys = csys[c];
   for (int t = threadIdx.x; t < K * ncols; t += kT) {
     const int kk = t / ncols, i = t % ncols;
-    cf[kk][i] = st.c(sys * K + kk)[i];
+    cf_c[kk * ncols + i] = st.c(sys * K + kk)[i];
   }
   if (threadIdx.x < K) ncq[threadIdx.x] = (int)st.misc(sys * K + threadIdx.x)[3];
   __syncthreads();
@@ -505,8 +511,8 @@ __global__ void __launch_bounds__(kT) b_combine(const int* crow, const int* csys
   for (long long e = e0 + threadIdx.x; e < e1; e += kT) {
     double s = 0.0;
     if (nck > 0) {
-      s = cf[k][0] * (double)V[e];
-      for (int i = 1; i < nck; ++i) s += cf[k][i] * (double)V[(long long)i * ld + e];
+      s = cf_c[k * ncols] * (double)V[e];
+      for (int i = 1; i < nck; ++i) s += cf_c[k * ncols + i] * (double)V[(long long)i * ld + e];
     }
     out[e] = s;
   }
@@ -760,9 +766,11 @@ struct BatchSolver {
       constexpr int G = VShape<K, T>::G > 2 ? 2 : VShape<K, T>::G;
       b_dots_v<K, T, G><<<dim3((j + G) / G, nch), kT, 0, s>>>(crow, csys, in, ld, j, V.get(), w.get(), red.get(), nch);
       DECO_CHECK_LAUNCH();
-      b_dots_fin<K><<<(int)cdiv(Q, kT / 32), kT, 0, s>>>(Q, sch, st, in, j, red.get(), nch);
+      b_dots_fin<K><<<(int)cdiv(Q, kT / 32), kT, sizeof(double) * (kT / 32) * (j + 1), s>>>(Q, sch, st, in, j,
+                                                                                            red.get(), nch);
       DECO_CHECK_LAUNCH();
-      b_update_v<K, T><<<nch, kT, 0, s>>>(crow, csys, st, in, ld, j, V.get(), w.get(), col(j + 1), red.get(), nch);
+      b_update_v<K, T><<<nch, kT, sizeof(double) * K * (j + 1), s>>>(crow, csys, st, in, ld, j, V.get(), w.get(),
+                                                                      col(j + 1), red.get(), nch);
       DECO_CHECK_LAUNCH();
       b_update_fin<K><<<qb, 128, 0, s>>>(Q, sch, st, in, j, red.get(), nch, prm.reltol, prm.itmax);
       DECO_CHECK_LAUNCH();
@@ -771,7 +779,7 @@ struct BatchSolver {
     }
     b_backsolve<K><<<qb, 128, 0, s>>>(Q, st, in, brk.get());
     DECO_CHECK_LAUNCH();
-    b_combine<K, T><<<nch, kT, 0, s>>>(crow, csys, st, ld, m, V.get(), xtmp.get());
+    b_combine<K, T><<<nch, kT, sizeof(double) * K * m, s>>>(crow, csys, st, ld, m, V.get(), xtmp.get());
     DECO_CHECK_LAUNCH();
     apply_outer(xtmp.get(), z64.get());
     b_axpy<<<grid_for(ctx, nk, 256), 256, 0, s>>>(nk, z64.get(), x);
@@ -1028,7 +1036,8 @@ int deco_batch_solve(deco_ctx ctx, deco_batch Bt, const double* d_B, double* d_X
   return guard([&] {
     DECO_REQUIRE(ctx && Bt && d_B && d_X && prm && res, DECO_ERR_ARG, "NULL argument");
     DECO_REQUIRE(prm->type == 0, DECO_ERR_UNSUPPORTED, "the batched solve runs rgmres");
-    DECO_REQUIRE(prm->restart >= 1 && prm->restart <= 63, DECO_ERR_UNSUPPORTED, "restart must be in [1, 63]");
+    DECO_REQUIRE(prm->restart >= 1 && prm->restart <= kMaxRestartB, DECO_ERR_UNSUPPORTED,
+                 "restart must be in [1, " + std::to_string(kMaxRestartB) + "]");
     DECO_REQUIRE(prm->itmax >= 0, DECO_ERR_ARG, "itmax must be >= 0");
     DECO_REQUIRE(prm->precision == Bt->P->prm.precision, DECO_ERR_ARG,
                  "solve precision must match the precision of the batch's CPR");

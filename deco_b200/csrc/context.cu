@@ -32,7 +32,10 @@ bool cache_on() {
 }
 }  // namespace
 
+std::atomic<long long> g_alloc_requests{0};
+
 void* dev_alloc(size_t bytes, cudaStream_t s, size_t* capacity) {
+  g_alloc_requests.fetch_add(1, std::memory_order_relaxed);
   if (cache_on() && bytes >= kCacheMin) {
     std::lock_guard<std::mutex> lk(g_cache_mu);
     auto it = g_cache.find(s);
@@ -252,6 +255,7 @@ extern "C" {
 const char* deco_last_error(void) { return g_last_error.c_str(); }
 const char* deco_version(void) { return "deco_b200 0.1 (sm_100a)"; }
 long long deco_launch_count(void) { return g_launches.load(); }
+long long deco_alloc_count(void) { return g_alloc_requests.load(); }
 
 int deco_ctx_create(int device, void* stream, deco_ctx* out) {
   return guard([&] {

@@ -476,6 +476,13 @@ static void cpr_build(deco_ctx_s* ctx, deco_csr_s* A, double* d_b, const deco_cp
   DECO_REQUIRE(A->n % bs == 0, DECO_ERR_ARG,
                "n is not divisible by bs, n = " + std::to_string(A->n) + ", bs = " + std::to_string(bs));
   DECO_REQUIRE(prm.pressure_id >= 0 && prm.pressure_id < bs, DECO_ERR_ARG, "pressure_id out of range");
+  // quasi_IMPES_GE (CPR.hpp:372-447) fills its (bs-1)x(bs-1) system at index
+  // (p - 1)(bs - 1) + column % bs - 1 for every row p != p_id and writes the
+  // weights to rows 1..bs-1 of the cell: with p_id != 0 row 0 lands at a negative
+  // index and the weight of row p_id is overwritten, so only p_id = 0 has a
+  // defined result to reproduce
+  DECO_REQUIRE(prm.weights != 2 || prm.pressure_id == 0, DECO_ERR_UNSUPPORTED,
+               "quasiimpes_GE weights need pressure_id 0 (the reference's quasi_IMPES_GE indexes from row 0)");
   DECO_REQUIRE(prm.seq >= 0 && prm.seq <= 3, DECO_ERR_ARG, "seq must be 0, 1, 2 or 3");
   DECO_REQUIRE((prm.glo_type == 0 || prm.glo_type == 1) && (prm.loc_type == 0 || prm.loc_type == 1),
                DECO_ERR_UNSUPPORTED, "prec_glo / prec_loc type must be FSAI or Jacobi on the GPU path");

@@ -14,15 +14,21 @@
 //   * the array lives as long as the library is loaded, on every device that
 //     loads it (8 MiB each);
 //   * the first call on a device resolves the array's device address with
-//     cudaGetSymbolAddress (with that device current) and caches it; make that
-//     first call before any stream capture;
+//     cudaGetSymbolAddress (with that device current) and caches it for the
+//     life of the process; make that first call before any stream capture.
+//     The cached address does not survive cudaDeviceReset (or any other
+//     destruction of the device's primary context): a process that resets a
+//     device must not call this entry point on it again;
 //   * all calls share the array and it keeps the last call's contents; nothing
 //     needs clearing, since the first product writes every entry before the
 //     second reads it;
 //   * calls that overlap on the GPU (two streams at once) race on the array;
 //   * the two products use the kernels deco_fsai_apply uses whenever those need no
-//     allocation (the padded copies), so the results agree with it; otherwise the
-//     CSR kernel at a width chosen without timing.
+//     allocation (the slot-padded copies), so the results are identical to its
+//     results then; a factor without padded copies goes through the CSR kernel
+//     at the heuristic width (no timing, no shared state), which sums in another
+//     order than the cell-block kernel deco_fsai_apply may pick: equal to
+//     rounding, not bit for bit.
 #include <map>
 #include <mutex>
 
@@ -57,12 +63,10 @@ void* scratch_address(int device) {
   return p;
 }
 
-// the matrix's chosen sub-warp width, or the heuristic one: never the timing
-// autotuner, which allocates
-int width_no_alloc(const deco_csr_s* A, bool f32) {
-  const int sw = f32 ? A->sw32 : A->sw64;
-  return sw ? sw : heuristic_subwarp(A->avg_row, f32 ? 4 : 2);
-}
+// the heuristic sub-warp width: never the timing autotuner, which allocates, nor
+// the width it caches on the matrix, which another thread's deco_fsai_apply may
+// be writing at the same time
+int width_no_alloc(const deco_csr_s* A, bool f32) { return heuristic_subwarp(A->avg_row, f32 ? 4 : 2); }
 
 // One factor product with the kernel deco_fsai_apply would pick when that needs no
 // allocation: the slot-padded copies (scalar rows, or 2x2 cell blocks with x

@@ -37,7 +37,18 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kMaxCols = kWarps * 8;  // basis columns pass A handles, 8 per warp (restart <= 63)
+// Largest restart length m.  The basis costs (m + 1) n words of HBM; the
+// kernels' per-column scratch (coefficients, one Hessenberg column, rotations)
+// lives in dynamic shared memory sized by the launch, so the bound only keeps
+// the dot pass's w/u_j tiles (32 KB) plus one column of coefficients (8 (m+1)
+// bytes) under the 48 KB a block gets without opting in.
+constexpr int kMaxRestart = 1000;
+constexpr int kColsF = kWarps * 4;  // columns one block row of the float32 dot pass takes (4 per warp)
+constexpr int kColsD = kWarps * 8;  // the same for the float64 register form (8 per warp)
+// back substitution with the triangle of H in shared memory up to this order
+// (j (j + 1) / 2 + j + 1 doubles, under the 227 KB opt-in limit); past it the
+// same arithmetic reads H from global memory
+constexpr int kBacksolveShm = 200;
 // host read-back of |g_{j+1}|: a ring of kRing pinned slots (from kSlot0) and
 // events; the host runs up to `lookahead` Arnoldi steps ahead (<= kRing - 2)
 constexpr int kRing = 8;
@@ -146,12 +157,12 @@ template <> struct Vec4<double> {
   __device__ static double get(const double2& a, int e) { return e == 0 ? a.x : a.y; }
 };
 
-// last block of pass A: h, the new Gram row, c = h + (h - G h) and H(:,j)
-__device__ void dots_finish(int ncols, int j, const double* __restrict__ red, State st) {
+// last block of pass A: h, the new Gram row, c = h + (h - G h) and H(:,j);
+// hs: ncols doubles of shared memory
+__device__ void dots_finish(int ncols, int j, const double* __restrict__ red, State st, double* hs) {
   finalize_partials(red, gridDim.x, 2 * ncols, st.sums);
   __syncthreads();
   // h_i = s_i (u_i . w);  G(i,j) = s_i s_j (u_i . u_j)
-  __shared__ double hs[kMaxCols];
   const double sj = st.s[j];
   for (int i = threadIdx.x; i < ncols; i += kThreads) {
     hs[i] = st.sums[i] * st.s[i];
@@ -197,9 +208,9 @@ __device__ __forceinline__ double vdot(const float4& a, const float4& b) {
 // the tiles of w and u_j are copied into shared memory (double-buffered cp.async,
 // so the next tile streams in while this one is used) and warp w streams columns
 // w, w+8, ... (CPW of them: the template is the smallest power of two with
-// 8*CPW >= ncols, at most 4; past 32 columns a second block per row range,
-// blockIdx.y = 1, takes columns 32..63) against them, keeping per-column
-// partial sums in registers.
+// 8*CPW >= ncols, at most 4; past 32 columns further blocks per row range,
+// blockIdx.y = 1, 2, ..., take columns 32..63, 64..95, ...) against them,
+// keeping per-column partial sums in registers.
 // Rows past the last full vector are summed by the last block.  (Measured on
 // B200, float32 basis, 8M rows, 26 columns: 168 us against 370 us when every
 // warp held w and u_j in registers and formed each product in float64; the
@@ -297,7 +308,8 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long 
     }
   }
   if (!last_block(counter)) return;
-  dots_finish(ncols, j, red, st);
+  extern __shared__ double dyn_hs[];
+  dots_finish(ncols, j, red, st, dyn_hs);
 }
 
 // ---- pass A for the float64 basis: the same dots with w and u_j held in
@@ -313,6 +325,7 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots_reg(long long n, long l
   using VT = typename Vec4<T>::t;
   constexpr int N = Vec4<T>::N;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int cbase = blockIdx.y * kColsD;  // block row y of the grid takes columns 64y .. 64y + 63
   const long long nvec = n / N;
   const long long per = (nvec + gridDim.x - 1) / gridDim.x;
   const long long v0 = per * blockIdx.x, v1 = min(nvec, v0 + per);
@@ -331,7 +344,7 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots_reg(long long n, long l
     }
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      const int c = warp + k * kWarps;
+      const int c = cbase + warp + k * kWarps;
       if (c < ncols) {
         const VT* __restrict__ vc = reinterpret_cast<const VT*>(V + (size_t)c * ld);
         VT v[kVecPerLane];
@@ -353,7 +366,7 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots_reg(long long n, long l
     for (long long r = nvec * N; r < n; ++r)
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
-        const int c = warp + k * kWarps;
+        const int c = cbase + warp + k * kWarps;
         if (c < ncols) {
           const double v = (double)V[(size_t)c * ld + r];
           pw[k] += v * (double)w[r];
@@ -363,7 +376,7 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots_reg(long long n, long l
   }
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    const int c = warp + k * kWarps;
+    const int c = cbase + warp + k * kWarps;
     const double a = warp_sum(pw[k]), b = warp_sum(pu[k]);
     if (lane == 0 && c < ncols) {
       red[(size_t)c * gridDim.x + blockIdx.x] = a;
@@ -371,29 +384,34 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots_reg(long long n, long l
     }
   }
   if (!last_block(counter)) return;
-  dots_finish(ncols, j, red, st);
+  extern __shared__ double dyn_hs[];
+  dots_finish(ncols, j, red, st, dyn_hs);
 }
 
 template <typename T>
 void launch_arnoldi_dots(cudaStream_t s, int nb, long long n, long long ld, int nc, int j, const T* V, const T* w,
                          double* red, unsigned* counter, State st) {
+  const size_t shm = sizeof(double) * (size_t)nc;  // h for the last block (dots_finish)
   if constexpr (std::is_same<T, double>::value)
-    arnoldi_dots_reg<T><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V, w, red, counter, st);
+    arnoldi_dots_reg<T><<<dim3(nb, (nc + kColsD - 1) / kColsD), kThreads, shm, s>>>(n, ld, nc, j, V, w, red, counter,
+                                                                                   st);
   else if (nc <= kWarps)
-    arnoldi_dots<T, 1><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V, w, red, counter, st);
+    arnoldi_dots<T, 1><<<nb, kThreads, shm, s>>>(n, ld, nc, j, V, w, red, counter, st);
   else if (nc <= 2 * kWarps)
-    arnoldi_dots<T, 2><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V, w, red, counter, st);
-  else if (nc <= 4 * kWarps)
-    arnoldi_dots<T, 4><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V, w, red, counter, st);
-  else  // two blocks per row range, 32 columns each: 56 registers instead of 76 for 8 columns per warp, at the
-        // cost of reading the w and u_j tiles twice (measured on the 8M-row system at restart 50: the
-        // orthogonalisation 0.343 against 0.353 ms per iteration)
-    arnoldi_dots<T, 4><<<dim3(nb, 2), kThreads, 0, s>>>(n, ld, nc, j, V, w, red, counter, st);
+    arnoldi_dots<T, 2><<<nb, kThreads, shm, s>>>(n, ld, nc, j, V, w, red, counter, st);
+  else  // 4 columns per warp; past 32 columns further blocks per row range, 32 columns each: 56 registers
+        // instead of 76 for 8 columns per warp, at the cost of reading the w and u_j tiles once per block row
+        // (measured on the 8M-row system at restart 50: the orthogonalisation 0.343 against 0.353 ms per
+        // iteration)
+    arnoldi_dots<T, 4><<<dim3(nb, (nc + kColsF - 1) / kColsF), kThreads, shm, s>>>(n, ld, nc, j, V, w, red, counter,
+                                                                                 st);
 }
 
 // ---- pass B: w'' = w - sum_c coef_c u_c, stored as column j+1; ||w''||^2.
 // One thread per 128-bit vector of rows; the column loop is unrolled so several
-// independent vector loads are in flight per thread.
+// independent vector loads are in flight per thread.  Dynamic shared memory:
+// 4 (ncols + 1) doubles (the coefficients, then column j of H and the earlier
+// rotations for the last block).
 template <typename T>
 __global__ void __launch_bounds__(kThreads) arnoldi_update(long long n, long long ld, int ncols, int j,
                                                            const T* __restrict__ V, const T* __restrict__ w,
@@ -401,7 +419,8 @@ __global__ void __launch_bounds__(kThreads) arnoldi_update(long long n, long lon
                                                            unsigned* counter, State st) {
   using VT = typename Vec4<T>::t;
   constexpr int N = Vec4<T>::N;
-  __shared__ double cs_[kMaxCols];
+  extern __shared__ double dyn_u[];
+  double* cs_ = dyn_u;
   for (int i = threadIdx.x; i < ncols; i += kThreads) cs_[i] = st.c[i];
   __syncthreads();
   const long long nvec = n / N;
@@ -444,7 +463,9 @@ __global__ void __launch_bounds__(kThreads) arnoldi_update(long long n, long lon
   finalize_partials(red, gridDim.x, 1, st.sc + SC_BETA);
   // the rotations run on a shared-memory copy of column j and of the earlier
   // rotations (one thread, a chain of j dependent updates)
-  __shared__ double hc[kMaxCols + 1], rc[kMaxCols], rs[kMaxCols];
+  double* hc = dyn_u + (ncols + 1);  // j + 2 entries
+  double* rc = hc + (ncols + 1);     // j entries
+  double* rs = rc + (ncols + 1);
   for (int i = threadIdx.x; i <= j; i += kThreads) hc[i] = st.h(i, j);
   for (int i = threadIdx.x; i < j; i += kThreads) { rc[i] = st.cs[i]; rs[i] = st.sn[i]; }
   __syncthreads();
@@ -506,20 +527,25 @@ __global__ void __launch_bounds__(kThreads) norm2_kernel(long long n, const X* _
 
 // back substitution g(1:j) = H(1:j,1:j) \ g(1:j)  (rgmres.tpp:95-104), then the
 // coefficients on the stored columns c_i = y_i s_i
-// One block: the upper triangle of H's first j columns and g are staged in
-// shared memory, then column by column g_i /= H(i,i) and, in parallel over k < i,
+// One block: the upper triangle of H's first j columns (packed by columns,
+// H(k,i) at i (i + 1) / 2 + k) and g are staged in dynamic shared memory when
+// SHM, then column by column g_i /= H(i,i) and, in parallel over k < i,
 // g_k -= H(k,i) g_i (every element sees the same operations in the same order as
-// the sequential column-oriented substitution).
+// the sequential column-oriented substitution).  Without SHM the same
+// arithmetic reads H from global memory (orders past kBacksolveShm).
+template <bool SHM>
 __global__ void __launch_bounds__(kThreads) backsolve(State st, int j) {
-  __shared__ double hs[(kMaxCols + 1) * kMaxCols];
-  __shared__ double g[kMaxCols + 1];
-  const int ldh = st.m + 1;
-  for (int i = 0; i < j; ++i)
-    for (int k = threadIdx.x; k <= i; k += kThreads) hs[k + i * ldh] = st.h(k, i);
+  extern __shared__ double dyn_b[];
+  double* g = dyn_b;       // j + 1 doubles
+  double* hs = g + j + 1;  // j (j + 1) / 2 doubles (SHM)
+  auto H = [&](int k, int i) -> double { return SHM ? hs[(size_t)i * (i + 1) / 2 + k] : st.h(k, i); };
+  if (SHM)
+    for (int i = 0; i < j; ++i)
+      for (int k = threadIdx.x; k <= i; k += kThreads) hs[(size_t)i * (i + 1) / 2 + k] = st.h(k, i);
   for (int k = threadIdx.x; k <= j; k += kThreads) g[k] = st.g[k];
   __syncthreads();
   for (int i = j - 1; i >= 0; --i) {
-    const double hii = hs[i + i * ldh];
+    const double hii = H(i, i);
     if (hii == 0.0) {  // the same value in every thread: the whole block leaves
       if (threadIdx.x == 0) st.sc[SC_BREAK] = 1.0;
       return;
@@ -527,13 +553,27 @@ __global__ void __launch_bounds__(kThreads) backsolve(State st, int j) {
     if (threadIdx.x == 0) g[i] /= hii;
     __syncthreads();
     const double gi = g[i];
-    for (int k = threadIdx.x; k < i; k += kThreads) g[k] -= hs[k + i * ldh] * gi;
+    for (int k = threadIdx.x; k < i; k += kThreads) g[k] -= H(k, i) * gi;
     __syncthreads();
   }
   if (threadIdx.x == 0) st.sc[SC_BREAK] = 0.0;
   for (int k = threadIdx.x; k <= j; k += kThreads) st.g[k] = g[k];
   const int nc = j > 0 ? j : 1;
   for (int i = threadIdx.x; i < nc; i += kThreads) st.c[i] = g[i] * st.s[i];
+}
+
+void launch_backsolve(cudaStream_t s, State st, int j) {
+  if (j <= kBacksolveShm) {
+    const size_t shm = sizeof(double) * ((size_t)j + 1 + (size_t)j * (j + 1) / 2);
+    if (shm > 48 * 1024) {
+      static_assert(sizeof(double) * (kBacksolveShm + 1 + kBacksolveShm * (kBacksolveShm + 1) / 2) <= 227 * 1024,
+                    "back-substitution triangle must fit the opt-in shared memory");
+      DECO_CUDA(cudaFuncSetAttribute(backsolve<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    }
+    backsolve<true><<<1, kThreads, shm, s>>>(st, j);
+  } else {
+    backsolve<false><<<1, kThreads, sizeof(double) * ((size_t)j + 1), s>>>(st, j);
+  }
 }
 
 // out = sum_{i < ncols} c_i u_i  (rgmres.tpp:106-109: w = g_0 v_0, then w += g_i v_i)
@@ -545,7 +585,7 @@ __global__ void __launch_bounds__(kThreads) combine(long long n, long long ld, i
   // sums in the same order as a row-by-row loop)
   using VT = typename Vec4<T>::t;
   constexpr int N = Vec4<T>::N;
-  __shared__ double cs[kMaxCols];
+  extern __shared__ double cs[];  // ncols doubles
   for (int i = threadIdx.x; i < ncols; i += kThreads) cs[i] = c[i];
   __syncthreads();
   const long long nvec = n / N;
@@ -709,8 +749,8 @@ struct Solver {
     const int nc = j + 1;
     launch_arnoldi_dots<T>(s, nb, n, ld, nc, j, V.get(), w.get(), ctx->red.get(), ctx->counter.get(), st);
     DECO_CHECK_LAUNCH();
-    arnoldi_update<T><<<nb, kThreads, 0, s>>>(n, ld, nc, j, V.get(), w.get(), col(j + 1), ctx->red.get(),
-                                              ctx->counter.get(), st);
+    arnoldi_update<T><<<nb, kThreads, sizeof(double) * 4 * (nc + 1), s>>>(n, ld, nc, j, V.get(), w.get(), col(j + 1),
+                                                                           ctx->red.get(), ctx->counter.get(), st);
     DECO_CHECK_LAUNCH();
     if (profile) DECO_CUDA(cudaEventRecord(pev[4 * j + 3], s));
     DECO_CUDA(cudaMemcpyAsync(const_cast<double*>(hsc) + kSlot0 + j % kRing, st.sc + SC_RES, sizeof(double),
@@ -776,14 +816,15 @@ struct Solver {
         ++j;
       }
       iter = base + j;
-      backsolve<<<1, kThreads, 0, s>>>(st, j);
+      launch_backsolve(s, st, j);
       DECO_CHECK_LAUNCH();
       DECO_CUDA(cudaMemcpyAsync(const_cast<double*>(hsc) + 3, st.sc + SC_BREAK, sizeof(double), cudaMemcpyDeviceToHost, s));
       DECO_CUDA(cudaStreamSynchronize(s));
       if (hsc[3] != 0.0)
         throw Error(DECO_ERR_BREAKDOWN, "Error in rgmres: Zero diagonal element in upper triangular matrix.");
       collect(launched);
-      combine<T, double><<<nb, kThreads, 0, s>>>(n, ld, j > 0 ? j : 1, V.get(), st.c, xtmp.get());
+      combine<T, double><<<nb, kThreads, sizeof(double) * (j > 0 ? j : 1), s>>>(n, ld, j > 0 ? j : 1, V.get(), st.c,
+                                                                                 xtmp.get());
       DECO_CHECK_LAUNCH();
       if (!left) {
         precond<double, double>(xtmp.get(), r);  // r is scratch for z here
@@ -841,8 +882,8 @@ int deco_gmres_solve(deco_ctx ctx, deco_csr A, deco_cpr P, const double* b, doub
     DECO_REQUIRE(ctx && A && b && x && prm && res, DECO_ERR_ARG, "NULL argument");
     DECO_REQUIRE(prm->type == 0 || prm->type == 1, DECO_ERR_ARG, "type must be 0 (rgmres) or 1 (lgmres)");
     DECO_REQUIRE(prm->restart >= 1, DECO_ERR_ARG, "restart must be >= 1");
-    DECO_REQUIRE(prm->restart < kMaxCols, DECO_ERR_UNSUPPORTED,
-                 "restart must be < " + std::to_string(kMaxCols) + " on this path");
+    DECO_REQUIRE(prm->restart <= kMaxRestart, DECO_ERR_UNSUPPORTED,
+                 "restart must be <= " + std::to_string(kMaxRestart) + " on this path");
     DECO_REQUIRE(prm->itmax >= 0, DECO_ERR_ARG, "itmax must be >= 0");
     DECO_REQUIRE(prm->precision == 64 || prm->precision == 32, DECO_ERR_ARG, "precision must be 64 or 32");
     DECO_REQUIRE(A->n == A->m, DECO_ERR_ARG, "A must be square");

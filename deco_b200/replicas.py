@@ -18,6 +18,15 @@ def shard(n_items: int, rank: int, world: int) -> range:
     return range(start, start + base + (1 if rank < extra else 0))
 
 
+def deal(n_items: int, rank: int, world: int) -> list[int]:
+    """Round-robin share of `n_items` independent systems for `rank`: items rank,
+    rank + world, ...  Systems of a batch are generated in random size order, so
+    dealing them spreads the large ones over the ranks (the batched bench's split)."""
+    if world < 1 or not (0 <= rank < world):
+        raise ValueError("bad rank/world")
+    return list(range(rank, n_items, world))
+
+
 def max_over_ranks(value: float, device=None) -> float:
     """All-reduce MAX of a per-rank scalar (identity without an initialised process group)."""
     import torch

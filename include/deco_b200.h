@@ -53,6 +53,11 @@ const char* deco_last_error(void);
 const char* deco_version(void);
 /* Kernels this library has launched in this process (all contexts). */
 long long deco_launch_count(void);
+/* Device-memory requests this library has made in this process (every request
+ * of its stream-ordered allocator, whether served from its block cache or by
+ * cudaMallocAsync).  No counterpart in the reference: a diagnostic, e.g. to
+ * check that deco_fsai_apply_static allocates nothing. */
+long long deco_alloc_count(void);
 
 /* ------------------------------------------------------------------ context
  * Replaces the reference's process-global state (MPI_Comm deco_comm,
@@ -218,7 +223,7 @@ int deco_cpr_decouple_rhs(deco_ctx ctx, deco_cpr P, double* d_b);
 typedef struct deco_sol_params {
   int type;              /* 0 rgmres, 1 lgmres                               */
   double reltol;         /* sol.reltol                                       */
-  int restart;           /* sol.restart                                      */
+  int restart;           /* sol.restart, 1..1000 (the reference allows any)  */
   int itmax;             /* sol.itmax (total inner iterations)               */
   int verbosity;         /* sol.verbosity                                    */
   int precision;         /* 64 or 32                                         */

@@ -73,7 +73,8 @@ def params_from_json(prec: dict) -> CprParams:
 def spmv(r, c, v, x, bs=1):
     n = len(r) - 1
     y = np.zeros((n + bs - 1) // bs)
-    lib().orc_spmv(n, _p(r), _p(c), _p(v), _p(np.ascontiguousarray(x, np.float64)), _p(y), bs)
+    xc = np.ascontiguousarray(x, np.float64)  # kept alive across the call
+    lib().orc_spmv(n, _p(r), _p(c), _p(v), _p(xc), _p(y), bs)
     return y
 
 
@@ -114,7 +115,8 @@ class Cpr:
 
     def apply(self, rvec):
         x = np.zeros(self.n)
-        lib().orc_cpr_apply(self.h, _p(np.ascontiguousarray(rvec, np.float64)), _p(x))
+        rc = np.ascontiguousarray(rvec, np.float64)  # kept alive across the call
+        lib().orc_cpr_apply(self.h, _p(rc), _p(x))
         return x
 
     def solve(self, sol: dict):

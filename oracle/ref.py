@@ -15,17 +15,36 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_ref", "libdeco_ref.so")
-REF_SRC = os.environ.get("DECO_REFERENCE", "/root/reference")
+# where the reference's sources are (a checkout of amavliut/deco); without it the
+# prebuilt oracle/_ref library is used as it is
+REF_SRC = os.environ.get("DECO_REFERENCE", "")
 
 _lib = None
 
 
-def build(quiet=True) -> bool:
-    """Compile the reference into oracle/_ref when its sources are present."""
-    if not os.path.isdir(REF_SRC):
+def openblas_dir() -> str:
+    """Directory of the OpenBLAS shared object that provides LAPACKE: DECO_OPENBLAS_DIR,
+    else the opencv wheel's bundled copy in this Python's site-packages."""
+    d = os.environ.get("DECO_OPENBLAS_DIR", "")
+    if d:
+        return d
+    import glob
+    import sysconfig
+    for base in {sysconfig.get_paths()["purelib"], sysconfig.get_paths()["platlib"]}:
+        hits = sorted(glob.glob(os.path.join(base, "opencv_python_headless.libs", "libopenblas*.so")))
+        if hits:
+            return os.path.dirname(hits[0])
+    raise RuntimeError("no OpenBLAS shared object found: set DECO_OPENBLAS_DIR to the directory of libopenblas*.so")
+
+
+def build(quiet=True, src: str | None = None) -> bool:
+    """Compile the reference into oracle/_ref from its sources at `src` (default
+    DECO_REFERENCE); without sources, report whether a prebuilt library exists."""
+    src = src or REF_SRC
+    if not src or not os.path.isdir(src):
         return os.path.exists(LIB)
-    subprocess.run(["make", "-s" if quiet else "-k", "-C", os.path.join(HERE, "ref"), f"REF={REF_SRC}"],
-                   check=True)
+    subprocess.run(["make", "-s" if quiet else "-k", "-C", os.path.join(HERE, "ref"), f"REF={src}",
+                    f"OBLASDIR={openblas_dir()}"], check=True)
     return os.path.exists(LIB)
 
 
@@ -88,7 +107,8 @@ def _p(a):
 def spmv(r, c, v, x, bs=1):
     n = len(r) - 1
     y = np.zeros((n + bs - 1) // bs, np.float64)
-    lib().ref_spmv(n, _p(r), _p(c), _p(v), _p(np.ascontiguousarray(x, np.float64)), _p(y), bs)
+    xc = np.ascontiguousarray(x, np.float64)  # kept alive across the call
+    lib().ref_spmv(n, _p(r), _p(c), _p(v), _p(xc), _p(y), bs)
     return y
 
 
@@ -121,7 +141,8 @@ class Fsai:
 
     def apply(self, x):
         y = np.empty(self.n)
-        lib().ref_fsai_apply(self.h, _p(np.ascontiguousarray(x, np.float64)), _p(y))
+        xc = np.ascontiguousarray(x, np.float64)  # kept alive across the call
+        lib().ref_fsai_apply(self.h, _p(xc), _p(y))
         return y
 
     def __del__(self):
@@ -170,7 +191,8 @@ class Cpr:
 
     def apply(self, rvec):
         x = np.zeros(self.n)
-        lib().ref_cpr_apply(self.h, _p(np.ascontiguousarray(rvec, np.float64)), _p(x))
+        rc = np.ascontiguousarray(rvec, np.float64)  # kept alive across the call
+        lib().ref_cpr_apply(self.h, _p(rc), _p(x))
         return x
 
     def solve(self, sol: dict | str):

@@ -19,7 +19,7 @@ def _built():
     build.build_gen()
     from oracle import port, ref
     port.build() if not os.path.exists(port.LIB) else None
-    if os.path.isdir(ref.REF_SRC):
+    if ref.REF_SRC and os.path.isdir(ref.REF_SRC):
         ref.build()
     yield
 

@@ -142,3 +142,64 @@ def test_driver_block_reorder(tmp_path):
     ref_it = port.Cpr(cpr_json(2), s.r, s.c, s.v, s.b).solve(sol)["iter"]
     assert abs(it - ref_it) <= max(1, 0.1 * ref_it) and res < 1e-8
     del rows
+
+
+@pytest.mark.gpu
+def test_driver_norne_parameters_restart_100(tmp_path):
+    """The shipped Norne parameter file's settings (param_norne.json): bs 3 with the
+    unknowns stored in 2-1-3 order (row_order / col_order "213"), quasiimpes_GE + DRS
+    (e_dd 0.2) + CPD, global FSAI with tol_rel 0.2, rgmres with restart 100, itmax 100
+    and reltol 1e-6, changed only in prec_loc (FSAI instead of hypre AMG, which stays on
+    the CPU build) and IO (binary files of a seeded 40x40x20 three-phase system with 1 %
+    fault connections instead of the Git-LFS sample).  Its one cycle runs past 64 basis
+    columns; the iteration count is within 10% of the reference build's on the
+    pressure-first system."""
+    from deco_b200 import gen
+    from oracle import ref
+    p = gen.preset(2, 1234)
+    p.nx, p.ny, p.nz = 40, 40, 20
+    s = gen.generate(p)
+    bs = 3
+    # stored order: position q of every cell holds original unknown perm[q] (2-1-3 order),
+    # which row_order / col_order "213" undo (adapter/csr2coo.cpp:18-86)
+    perm = np.array([1, 0, 2])
+    sw = lambda i: i - i % bs + perm[i % bs]
+    rows_st = sw(np.arange(s.n))
+    r2 = np.zeros(s.n + 1, np.int64)
+    np.cumsum(np.diff(s.r)[rows_st], out=r2[1:])
+    c2, v2 = np.empty_like(s.c), np.empty_like(s.v)
+    inv = np.argsort(perm)
+    swc = lambda i: i - i % bs + inv[i % bs]
+    for i in range(s.n):
+        a, e = s.r[rows_st[i]], s.r[rows_st[i] + 1]
+        cc, vv = swc(s.c[a:e]), s.v[a:e]
+        o = np.argsort(cc, kind="stable")
+        c2[r2[i]:r2[i + 1]], v2[r2[i]:r2[i + 1]] = cc[o], vv[o]
+    fa, fb = tmp_path / "A.bin", tmp_path / "b.bin"
+    with open(fa, "wb") as f:
+        np.array([s.n, s.n, s.nnz], np.int32).tofile(f)
+        r2.astype(np.int32).tofile(f); c2.astype(np.int32).tofile(f); v2.tofile(f)
+    with open(fb, "wb") as f:
+        np.array([s.n], np.int32).tofile(f)
+        s.b[rows_st].tofile(f)
+    prec = {"type": "CPR", "verbosity": "0", "row_order": "213", "col_order": "213", "block_size": "3",
+            "pressure_id": "0", "seq": "3", "weights": "quasiimpes_GE", "use_drs": "1",
+            "drs": {"e_dd": "0.2", "e_ps": "0.0"}, "CPD": "1", "tol_zero": "0.0",
+            "prec_glo": {"type": "FSAI", "input_file": "optional", "tol_rel": "0.2", "tol_abs": "1e-16",
+                         "verbosity": "0", "power": "1", "block_size": "1"},
+            "prec_loc": {"type": "FSAI", "tol_rel": "1e-4", "tol_abs": "1e-16", "power": "1", "block_size": "1"}}
+    sol = {"type": "rgmres", "input_file": "optional", "reltol": "1e-6", "restart": "100", "itmax": "100",
+           "verbosity": "1"}
+    io = {"file_A": str(fa), "file_b": str(fb), "header": "1", "format": "bin", "write": "0",
+          "wfile_x": str(tmp_path / "x.bin")}
+    rc, it, res, out = run(write_params(tmp_path, io, prec, sol))
+    assert rc == 0, out.stderr
+    ref_prec = {k: v for k, v in prec.items() if k not in ("row_order", "col_order")}
+    R = ref.Cpr({"prec": ref_prec}, s.r, s.c, s.v, s.b)
+    rres = R.solve(dict(sol, verbosity="0"))
+    assert rres["iter"] > 64 and rres["flag"] == 0
+    assert abs(it - rres["iter"]) <= max(1, 0.1 * rres["iter"]), (it, rres["iter"])
+    assert res < 1e-6
+    # x is written in the reordered (pressure-first) order, that of the reference's system
+    x = np.fromfile(tmp_path / "x.bin", dtype=np.float64, offset=4)
+    assert np.linalg.norm(x - rres["x"]) / np.linalg.norm(rres["x"]) < 1e-4

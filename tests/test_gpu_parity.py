@@ -205,6 +205,56 @@ def test_cpr_setup_and_apply(d, oracle, name, case):
     assert rel(x, R.apply(rv)) < 1e-12
 
 
+@pytest.mark.parametrize("name", ["c1", "bs3_faults"])
+@pytest.mark.parametrize("weights", ["quasiimpes", "none"])
+def test_cpr_pressure_id_1_matches_reference(d, oracle, name, weights):
+    """pressure_id 1 (CPR.hpp:50): the quasi-IMPES weights solve B^T w = e_1 (CPR.hpp:336),
+    A_pp is the in-block row/column 1 (local_matrix, CSR.hpp:338-420), and the apply
+    restricts r at row s*bs+1 against the row-0 product and prolongs into row s*bs+1
+    (CPR.hpp:241-256; fix_diag and IMPES keep their default row 0).  Against the reference
+    build: pattern bit-exact, values equal (1e-13 for the LAPACK weights), apply 1e-12.
+    With quasi-IMPES weights on these pressure-first systems the reference's own global
+    FSAI factor holds non-finite values (its local systems turn singular once row 0 gets
+    the weighted sum and row 1 the pressure role), so its apply is NaN there and only the
+    setup is compared."""
+    _, ref = oracle
+    s = system(name)
+    prec = cpr_json(s.bs, weights=weights)
+    prec["pressure_id"] = "1"
+    A = d.CSR.from_system(s)
+    b = cuda(s.b)
+    P = d.CPR(prec, A, b)
+    R = ref.Cpr({"prec": prec}, s.r, s.c, s.v, s.b)
+    r, c, v = A.download()
+    Rr, Rc, Rv, Rb = R.decoupled()
+    np.testing.assert_array_equal(r, Rr)
+    np.testing.assert_array_equal(c, Rc)
+    if weights == "none":
+        np.testing.assert_array_equal(v, Rv)
+        np.testing.assert_array_equal(b.cpu().numpy(), Rb)
+    else:
+        assert rel(v, Rv) < 1e-13 and rel(b.cpu().numpy(), Rb) < 1e-13
+    pr, pc, pv = P.Ap.download()
+    Rpr, Rpc, Rpv = R.pressure()
+    np.testing.assert_array_equal(pr, Rpr)
+    np.testing.assert_array_equal(pc, Rpc)
+    assert rel(pv, Rpv) < 1e-13
+    if weights == "none":
+        rv = np.random.default_rng(17).standard_normal(s.n)
+        assert rel(P.apply(cuda(rv)).cpu().numpy(), R.apply(rv)) < 1e-12
+
+
+def test_cpr_pressure_id_quasiimpes_ge_refused(d):
+    """quasi_IMPES_GE writes its 1x1 / 2x2 system from row 0 (CPR.hpp:402-409, 433-437): with
+    pressure_id != 0 the reference indexes out of bounds, so the GPU path refuses it."""
+    s = system("tiny")
+    prec = cpr_json(2)
+    prec["pressure_id"] = "1"
+    with pytest.raises(d.DecoError) as e:
+        d.CPR(prec, d.CSR.from_system(s), cuda(s.b))
+    assert e.value.code == -6
+
+
 def test_cpr_fix_diag_zero_saturation_diagonal(d, oracle):
     """fix_diag (CPR.hpp:753-840): zero saturation diagonals are replaced, then undone."""
     port, _ = oracle
@@ -272,22 +322,77 @@ def test_gmres_matches_reference(d, oracle, name, stype):
     assert rel(x, res["x"]) < 1e-6
 
 
-def test_gmres_mixed_precision_reaches_fp64_residual(d, oracle):
-    """precision 32: float32 CPR + float32 Krylov basis, float64 refinement."""
+@pytest.mark.parametrize("stype", ["rgmres", "lgmres"])
+@pytest.mark.parametrize("precision", [64, 32])
+def test_gmres_restart_100_matches_reference(d, oracle, stype, precision):
+    """restart 100, as every shipped parameter file sets it (param_norne.json:15): cycles
+    longer than 64 columns (several block rows in the dot pass, the back substitution's
+    triangle in opt-in shared memory).  Float64: iterations within 10% of the reference
+    build's, x within 1e-6 of the reference's.  Mixed precision is iterative refinement:
+    a float32 cycle cannot carry the true residual more than about six decades below the
+    residual it started from, so a solve that the float64 path finishes inside one or two
+    long cycles may need one more refinement cycle; the bar is the reference's count plus
+    one restart cycle, x within 1e-5.  Right GMRES: float64 true residual below 1e-8."""
     port, ref = oracle
     s = system("c1")
+    prec = cpr_json(s.bs)
+    sol = sol_json(stype, restart=100)
+    A = d.CSR.from_system(s)
+    b = cuda(s.b)
+    P = d.CPR(prec, A, b, precision=precision)
+    S = d.SOL(sol, A, P, b, precision=precision)
+    R = ref.Cpr({"prec": prec}, s.r, s.c, s.v, s.b)
+    res = R.solve(sol)
+    assert res["iter"] > 64, "the case must run cycles longer than 64 columns"
+    assert S.flag == 0 and res["flag"] == 0
+    if precision == 64:
+        assert abs(S.iter - res["iter"]) <= max(1, 0.1 * res["iter"]), (S.iter, res["iter"])
+    else:
+        assert S.iter <= res["iter"] + 100, (S.iter, res["iter"])
+    Dr, Dc, Dv, Db = R.decoupled()
+    x = S.x.cpu().numpy()
+    if stype == "rgmres":
+        true_rel = np.linalg.norm(Db - port.spmv(Dr, Dc, Dv, x)) / np.linalg.norm(Db)
+        assert true_rel < 1e-8
+    err = rel(x, res["x"])
+    print(f"restart 100 {stype} precision {precision}: {S.iter} iterations (reference {res['iter']}), "
+          f"|x - x_ref| / |x_ref| = {err:.2e}")
+    assert err < (1e-6 if precision == 64 else 1e-5)
+
+
+@pytest.mark.parametrize("name", ["c1", "bs3_faults"])
+def test_gmres_mixed_precision_reaches_fp64_residual(d, oracle, name):
+    """precision 32: float32 CPR + float32 Krylov basis, float64 refinement.  The
+    float64 true residual reaches 1e-8 and the error of the mixed solution against the
+    reference's float64 solution is stated and below 1e-6 (relative, 2-norm).  The
+    iteration count is within 10% of the reference's float64 count when the solve spans
+    several restart cycles (c1: about 220 iterations; the 1.5M- and 8M-row systems are
+    held to the same bar in test_gpu_configs.py).  A solve that the float64 path
+    finishes inside one cycle (bs3_faults: 25 iterations) takes one more refinement
+    cycle in mixed precision -- a float32 cycle does not carry the true residual from 1 to
+    1e-8 -- so there the bar is the float64 count plus one restart cycle."""
+    port, ref = oracle
+    s = system(name)
     prec = cpr_json(s.bs)
     A = d.CSR.from_system(s)
     b = cuda(s.b)
     P = d.CPR(prec, A, b, precision=32)
     S = d.SOL(sol_json(), A, P, b, precision=32)
     R = ref.Cpr({"prec": prec}, s.r, s.c, s.v, s.b)
-    ref_it = R.solve(sol_json())["iter"]
+    res = R.solve(sol_json())
+    ref_it = res["iter"]
     Dr, Dc, Dv, Db = R.decoupled()
     x = S.x.cpu().numpy()
     true_rel = np.linalg.norm(Db - port.spmv(Dr, Dc, Dv, x)) / np.linalg.norm(Db)
+    err = rel(x, res["x"])
+    print(f"mixed {name}: {S.iter} iterations (reference float64 {ref_it}), true residual {true_rel:.2e}, "
+          f"|x_mixed - x_ref| / |x_ref| = {err:.2e}")
     assert S.flag == 0 and true_rel < 1e-8
-    assert S.iter <= 2 * ref_it
+    if ref_it > 50:
+        assert abs(S.iter - ref_it) <= max(1, 0.1 * ref_it), (S.iter, ref_it)
+    else:
+        assert S.iter <= ref_it + 50, (S.iter, ref_it)
+    assert err < 1e-6
 
 
 ORIG_CASES = {

@@ -40,11 +40,46 @@ def test_static_scratch_apply_matches_the_allocating_apply(d, precision):
         x = torch.from_numpy(rng.standard_normal(s.n)).cuda()
         want = F.apply(x)
         got = torch.full_like(x, float("nan"))
+        before = L.deco_alloc_count()
         rc = L.deco_fsai_apply_static(d.default_context().h, F.h, _ptr(x), _ptr(got))
         assert rc == 0, L.deco_last_error().decode()
+        assert L.deco_alloc_count() == before, "the static apply asked the library's allocator for memory"
         torch.cuda.synchronize()
         err = ((got - want).norm() / want.norm()).item()
         assert err < 1e-12, err
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_static_scratch_apply_without_padded_copies(d, precision):
+    """With the slot-padded copies switched off (DECO_PADDED=0 at context creation)
+    the static apply takes the CSR kernel at the heuristic width, while the
+    allocating apply may take the cell-block kernel: the same products summed in
+    another order, equal to rounding (1e-12 float64; 1e-6 for the float32 factor,
+    whose float32 partial sums differ by a few float32 roundings)."""
+    import os
+    from deco_b200 import _lib, gen
+    L = _lib.lib()
+    os.environ["DECO_PADDED"] = "0"
+    try:
+        ctx = d.Context(0)
+    finally:
+        os.environ.pop("DECO_PADDED", None)
+    s = gen.generate(gen.preset(1))
+    A = d.CSR.from_system(s, ctx)
+    F = d.FSAI({"tol_rel": 0.0, "tol_abs": 1e-16, "power": 1}, A, precision=precision)
+    assert F.padded == (0, 0)
+    rng = np.random.default_rng(23)
+    for _ in range(2):
+        x = torch.from_numpy(rng.standard_normal(s.n)).cuda()
+        want = F.apply(x)
+        got = torch.full_like(x, float("nan"))
+        before = L.deco_alloc_count()
+        rc = L.deco_fsai_apply_static(ctx.h, F.h, _ptr(x), _ptr(got))
+        assert rc == 0, L.deco_last_error().decode()
+        assert L.deco_alloc_count() == before
+        ctx.sync()
+        err = ((got - want).norm() / want.norm()).item()
+        assert err < (1e-12 if precision == 64 else 1e-6), err
 
 
 def test_static_scratch_apply_refuses_too_many_rows(d):
