@@ -363,11 +363,24 @@ __global__ void __launch_bounds__(kT) b_update_v(const int* crow, const int* csy
   double ss[E];
 #pragma unroll
   for (int q = 0; q < E; ++q) ss[q] = 0.0;
+  // the columns go in batches of UB whose loads are all issued before their
+  // products (UB independent loads per thread in flight; each element still
+  // subtracts the columns in order)
+  constexpr int UB = sizeof(T) == 4 ? 16 : 8;
   for (long long f = f0 + threadIdx.x; f < f1; f += kT) {
     double x[E];
     vload<T, E>(w + f * E, x, false);
-#pragma unroll 4
-    for (int i = 0; i < nc; ++i) {
+    int i = 0;
+    for (; i + UB <= nc; i += UB) {
+      double v[UB][E];
+#pragma unroll
+      for (int u = 0; u < UB; ++u) vload<T, E>(V + (long long)(i + u) * ld + f * E, v[u], true);
+#pragma unroll
+      for (int u = 0; u < UB; ++u)
+#pragma unroll
+        for (int q = 0; q < E; ++q) x[q] -= cf_u[(i + u) * K + E * ph + q] * v[u][q];
+    }
+    for (; i < nc; ++i) {
       double v[E];
       vload<T, E>(V + (long long)i * ld + f * E, v, true);
 #pragma unroll

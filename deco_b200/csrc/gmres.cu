@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <mutex>
 #include <type_traits>
 #include <vector>
 
@@ -39,12 +40,11 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 // Largest restart length m.  The basis costs (m + 1) n words of HBM; the
 // kernels' per-column scratch (coefficients, one Hessenberg column, rotations)
-// lives in dynamic shared memory sized by the launch, so the bound only keeps
-// the dot pass's w/u_j tiles (32 KB) plus one column of coefficients (8 (m+1)
-// bytes) under the 48 KB a block gets without opting in.
+// lives in dynamic shared memory sized by the launch; the bound keeps the float32
+// dot pass's stages (64 KB) plus one column of coefficients (8 (m+1) bytes) well
+// inside a block's shared memory.
 constexpr int kMaxRestart = 1000;
-constexpr int kColsF = kWarps * 4;  // columns one block row of the float32 dot pass takes (4 per warp)
-constexpr int kColsD = kWarps * 8;  // the same for the float64 register form (8 per warp)
+constexpr int kColsD = kWarps * 8;  // columns one block row of the dot pass takes (8 per warp)
 // back substitution with the triangle of H in shared memory up to this order
 // (j (j + 1) / 2 + j + 1 doubles, under the 227 KB opt-in limit); past it the
 // same arithmetic reads H from global memory
@@ -204,90 +204,98 @@ __device__ __forceinline__ double vdot(const float4& a, const float4& b) {
 }
 
 // ---- pass A: raw dots u_c . w and u_c . u_j for c < ncols (u = stored columns).
-// Blocks own contiguous ranges of 128-bit vectors, walked in tiles of kTileVec;
-// the tiles of w and u_j are copied into shared memory (double-buffered cp.async,
-// so the next tile streams in while this one is used) and warp w streams columns
-// w, w+8, ... (CPW of them: the template is the smallest power of two with
-// 8*CPW >= ncols, at most 4; past 32 columns further blocks per row range,
-// blockIdx.y = 1, 2, ..., take columns 32..63, 64..95, ...) against them,
-// keeping per-column partial sums in registers.
-// Rows past the last full vector are summed by the last block.  (Measured on
-// B200, float32 basis, 8M rows, 26 columns: 168 us against 370 us when every
-// warp held w and u_j in registers and formed each product in float64; the
-// float32 conversions, not the loads, bounded that form.)
-constexpr int kTileVec = 512;
+// Blocks own contiguous ranges of 128-bit vectors, walked in chunks of
+// kChunk = 32 * kVecPerLane vectors (kVecPerLane per lane).  Warp w streams
+// columns w, w+8, ... (CPW of them: the smallest power of two with 8*CPW >= ncols,
+// at most 8; past 64 columns further blocks per row range, blockIdx.y = 1, 2, ...,
+// take columns 64..127, ...) against w and u_j, keeping per-column partial sums
+// in registers.  The column chunks reach the warp through a private ring of
+// kStages shared-memory stages filled by cp.async kStages - 1 chunks ahead, so
+// the loads in flight hold no registers and no block barrier paces the warps;
+// each lane reads back only the vectors it copied itself.  w and u_j, which every
+// warp of the block needs, are read per chunk through L1.  Rows past the last full
+// vector are summed by the last block.  (Measured on B200, float32 basis, 8M rows,
+// restart 50, every step of a cycle: 0.160 ms per step against 0.170 ms with
+// double-buffered w/u_j tiles and registers for the column loads; an update pass
+// of the same bytes runs at 0.135 ms.)
 constexpr int kVecPerLane = 4;
+constexpr int kChunk = 32 * kVecPerLane;
+constexpr int kStages = 4;
+constexpr size_t kDotsStageBytes = (size_t)kWarps * kStages * kChunk * 16;  // 64 KB per block
 template <typename T, int CPW>  // T = float
 __global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long ld, int ncols, int j,
                                                          const T* __restrict__ V, const T* __restrict__ w,
                                                          double* __restrict__ red, unsigned* counter, State st) {
-  using VT = typename Vec4<T>::t;
-  constexpr int N = Vec4<T>::N;
-  static_assert(kTileVec % (32 * kVecPerLane) == 0, "tile must hold whole lane steps");
-  __shared__ __align__(16) VT ws[2][kTileVec];
-  __shared__ __align__(16) VT us[2][kTileVec];
+  static_assert(std::is_same<T, float>::value, "the staged dot pass is the float32-basis form");
+  extern __shared__ __align__(16) unsigned char dots_smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int cbase = blockIdx.y * (kWarps * CPW);  // a second block row of the grid takes the next columns
-  const long long nvec = n / N;
+  float4* stg = reinterpret_cast<float4*>(dots_smem) + (size_t)warp * kStages * kChunk;
+  double* hs = reinterpret_cast<double*>(dots_smem + kDotsStageBytes);  // ncols doubles for dots_finish
+  const int cbase = blockIdx.y * (kWarps * CPW);
+  int nk = 0;  // columns of this warp (uniform over its lanes)
+#pragma unroll
+  for (int k = 0; k < CPW; ++k) nk += (cbase + warp + k * kWarps < ncols) ? 1 : 0;
+  const long long nvec = n / 4;
   const long long per = (nvec + gridDim.x - 1) / gridDim.x;
   const long long v0 = min(nvec, per * blockIdx.x), v1 = min(nvec, v0 + per);
-  const VT* __restrict__ wv4 = reinterpret_cast<const VT*>(w);
-  const VT* __restrict__ uv4 = reinterpret_cast<const VT*>(V + (size_t)j * ld);
-  double pw[CPW], pu[CPW];
+  const float4* __restrict__ wv4 = reinterpret_cast<const float4*>(w);
+  const float4* __restrict__ uv4 = reinterpret_cast<const float4*>(V + (size_t)j * ld);
+  // a block's row range is a few dozen chunks: 32-bit bookkeeping, advanced
+  // incrementally (no division per unit)
+  const int nch = (int)((v1 - v0 + kChunk - 1) / kChunk);
+  // the producer cursor: next (chunk, column) unit to copy and its stage; one
+  // commit group per unit (empty past the end) keeps the wait_group count uniform
+  int pch = 0, pk = 0, pst = 0;
+  auto issue = [&]() {
+    if (pch < nch) {
+      const float4* __restrict__ vc = reinterpret_cast<const float4*>(V + (size_t)(cbase + warp + pk * kWarps) * ld);
+      float4* dst = stg + pst * kChunk;
+      const long long c0 = v0 + (long long)pch * kChunk + lane;
 #pragma unroll
-  for (int k = 0; k < CPW; ++k) { pw[k] = 0.0; pu[k] = 0.0; }
-  const int ntiles = (int)((v1 - v0 + kTileVec - 1) / kTileVec);
-  auto load_tile = [&](int t, int buf) {
-    const long long t0 = v0 + (long long)t * kTileVec;
-    for (int i = threadIdx.x; i < kTileVec; i += kThreads) {
-      const long long vi = t0 + i;
-      if (vi < v1) {
-        cp_async16(&ws[buf][i], wv4 + vi);
-        cp_async16(&us[buf][i], uv4 + vi);
-      } else {
-        ws[buf][i] = Vec4<T>::zero();
-        us[buf][i] = Vec4<T>::zero();
-      }
+      for (int q = 0; q < kVecPerLane; ++q)
+        if (c0 + q * 32 < v1) cp_async16(dst + q * 32 + lane, vc + c0 + q * 32);
+      if (++pk == nk) { pk = 0; ++pch; }
+      if (++pst == kStages) pst = 0;
     }
     cp_async_commit();
   };
-  if (ntiles > 0) load_tile(0, 0);
-  for (int t = 0; t < ntiles; ++t) {
-    const int buf = t & 1;
-    if (t + 1 < ntiles) {
-      load_tile(t + 1, buf ^ 1);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+  double pw[CPW], pu[CPW];
+#pragma unroll
+  for (int k = 0; k < CPW; ++k) { pw[k] = 0.0; pu[k] = 0.0; }
+  if (nk > 0) {
+#pragma unroll
+    for (int i = 0; i < kStages - 1; ++i) issue();
+  }
+  int cst = 0;  // the consumer's stage
+  for (int ch = 0; ch < nch && nk > 0; ++ch) {
+    const long long c0 = v0 + (long long)ch * kChunk + lane;
+    float4 wv[kVecPerLane], uv[kVecPerLane];
+#pragma unroll
+    for (int q = 0; q < kVecPerLane; ++q) {
+      const bool in = c0 + q * 32 < v1;
+      wv[q] = in ? __ldg(wv4 + c0 + q * 32) : make_float4(0.f, 0.f, 0.f, 0.f);
+      uv[q] = in ? __ldg(uv4 + c0 + q * 32) : make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    __syncthreads();
-    const long long t0 = v0 + (long long)t * kTileVec;
 #pragma unroll
     for (int k = 0; k < CPW; ++k) {
-      const int c = cbase + warp + k * kWarps;
-      if (c < ncols) {
-        const VT* __restrict__ vc = reinterpret_cast<const VT*>(V + (size_t)c * ld);
-        for (int s0 = 0; s0 < kTileVec; s0 += 32 * kVecPerLane) {
-          VT v[kVecPerLane];
+      if (k < nk) {
+        issue();
+        cp_async_wait<kStages - 1>();  // this lane's copies of the unit (ch, k) have landed
+        const float4* src = stg + cst * kChunk;
+        if (++cst == kStages) cst = 0;
 #pragma unroll
-          for (int q = 0; q < kVecPerLane; ++q) {
-            const long long vi = t0 + s0 + lane + 32 * q;
-            v[q] = vi < v1 ? __ldcs(vc + vi) : Vec4<T>::zero();
-          }
-#pragma unroll
-          for (int q = 0; q < kVecPerLane; ++q) {
-            const int si = s0 + lane + 32 * q;
-            pw[k] += vdot(v[q], ws[buf][si]);
-            pu[k] += vdot(v[q], us[buf][si]);
-          }
+        for (int q = 0; q < kVecPerLane; ++q) {
+          const float4 v = c0 + q * 32 < v1 ? src[q * 32 + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+          pw[k] += vdot(v, wv[q]);
+          pu[k] += vdot(v, uv[q]);
         }
       }
     }
-    __syncthreads();  // buffer `buf` is refilled by the next iteration's copy
   }
+  cp_async_wait<0>();
   if (blockIdx.x == gridDim.x - 1 && lane == 0) {  // rows past the last full vector
     const T* __restrict__ uj = V + (size_t)j * ld;
-    for (long long r = nvec * N; r < n; ++r)
+    for (long long r = nvec * 4; r < n; ++r)
 #pragma unroll
       for (int k = 0; k < CPW; ++k) {
         const int c = cbase + warp + k * kWarps;
@@ -308,8 +316,7 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long 
     }
   }
   if (!last_block(counter)) return;
-  extern __shared__ double dyn_hs[];
-  dots_finish(ncols, j, red, st, dyn_hs);
+  dots_finish(ncols, j, red, st, hs);
 }
 
 // ---- pass A for the float64 basis: the same dots with w and u_j held in
@@ -388,30 +395,59 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots_reg(long long n, long l
   dots_finish(ncols, j, red, st, dyn_hs);
 }
 
+// the staged float32 dot pass needs more than the 48 KB of shared memory a block
+// gets by default: raise the limit once per (instantiation, device)
+template <int CPW>
+void allow_dots_smem() {
+  static std::mutex mu;
+  static std::vector<int> done;
+  int dev = 0;
+  DECO_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)done.size() <= dev) done.resize(dev + 1, 0);
+  if (done[dev]) return;
+  DECO_CUDA(cudaFuncSetAttribute(arnoldi_dots<float, CPW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(kDotsStageBytes + sizeof(double) * (kMaxRestart + 1))));
+  done[dev] = 1;
+}
+
 template <typename T>
 void launch_arnoldi_dots(cudaStream_t s, int nb, long long n, long long ld, int nc, int j, const T* V, const T* w,
                          double* red, unsigned* counter, State st) {
   const size_t shm = sizeof(double) * (size_t)nc;  // h for the last block (dots_finish)
-  if constexpr (std::is_same<T, double>::value)
+  if constexpr (std::is_same<T, double>::value) {
     arnoldi_dots_reg<T><<<dim3(nb, (nc + kColsD - 1) / kColsD), kThreads, shm, s>>>(n, ld, nc, j, V, w, red, counter,
                                                                                    st);
-  else if (nc <= kWarps)
-    arnoldi_dots<T, 1><<<nb, kThreads, shm, s>>>(n, ld, nc, j, V, w, red, counter, st);
-  else if (nc <= 2 * kWarps)
-    arnoldi_dots<T, 2><<<nb, kThreads, shm, s>>>(n, ld, nc, j, V, w, red, counter, st);
-  else  // 4 columns per warp; past 32 columns further blocks per row range, 32 columns each: 56 registers
-        // instead of 76 for 8 columns per warp, at the cost of reading the w and u_j tiles once per block row
-        // (measured on the 8M-row system at restart 50: the orthogonalisation 0.343 against 0.353 ms per
-        // iteration)
-    arnoldi_dots<T, 4><<<dim3(nb, (nc + kColsF - 1) / kColsF), kThreads, shm, s>>>(n, ld, nc, j, V, w, red, counter,
-                                                                                 st);
+  } else {
+    // two blocks per SM of 64 KB stages each (measured at restart 50 on 8M rows:
+    // 0.160 ms per step against 0.170 with three blocks per SM)
+    const int nbd = nb / 2;
+    const size_t shs = kDotsStageBytes + shm;
+    if (nc <= kWarps) {
+      allow_dots_smem<1>();
+      arnoldi_dots<T, 1><<<nbd, kThreads, shs, s>>>(n, ld, nc, j, V, w, red, counter, st);
+    } else if (nc <= 2 * kWarps) {
+      allow_dots_smem<2>();
+      arnoldi_dots<T, 2><<<nbd, kThreads, shs, s>>>(n, ld, nc, j, V, w, red, counter, st);
+    } else if (nc <= 4 * kWarps) {
+      allow_dots_smem<4>();
+      arnoldi_dots<T, 4><<<nbd, kThreads, shs, s>>>(n, ld, nc, j, V, w, red, counter, st);
+    } else {  // 8 columns per warp; past 64 columns further block rows, 64 columns each
+      allow_dots_smem<8>();
+      arnoldi_dots<T, 8><<<dim3(nbd, (nc + kColsD - 1) / kColsD), kThreads, shs, s>>>(n, ld, nc, j, V, w, red,
+                                                                                      counter, st);
+    }
+  }
 }
 
 // ---- pass B: w'' = w - sum_c coef_c u_c, stored as column j+1; ||w''||^2.
-// One thread per 128-bit vector of rows; the column loop is unrolled so several
-// independent vector loads are in flight per thread.  Dynamic shared memory:
-// 4 (ncols + 1) doubles (the coefficients, then column j of H and the earlier
-// rotations for the last block).
+// One thread per 128-bit vector of rows; the columns go in batches of U whose
+// loads are all issued before their products, so U independent 16-byte loads
+// per thread are in flight (U = 16 float32 / 8 float64; each element still
+// subtracts the columns in order).  Measured on B200, float32 basis, 8M rows,
+// restart 50: 0.135 ms per step against 0.152 ms with the column loop unrolled by 4.
+// Dynamic shared memory: 4 (ncols + 1) doubles (the coefficients, then column j
+// of H and the earlier rotations for the last block).
 template <typename T>
 __global__ void __launch_bounds__(kThreads) arnoldi_update(long long n, long long ld, int ncols, int j,
                                                            const T* __restrict__ V, const T* __restrict__ w,
@@ -419,6 +455,7 @@ __global__ void __launch_bounds__(kThreads) arnoldi_update(long long n, long lon
                                                            unsigned* counter, State st) {
   using VT = typename Vec4<T>::t;
   constexpr int N = Vec4<T>::N;
+  constexpr int U = N == 4 ? 16 : 8;
   extern __shared__ double dyn_u[];
   double* cs_ = dyn_u;
   for (int i = threadIdx.x; i < ncols; i += kThreads) cs_[i] = st.c[i];
@@ -431,8 +468,19 @@ __global__ void __launch_bounds__(kThreads) arnoldi_update(long long n, long lon
     double x[N];
 #pragma unroll
     for (int e = 0; e < N; ++e) x[e] = Vec4<T>::get(wv, e);
-#pragma unroll 4
-    for (int i = 0; i < ncols; ++i) {
+    int i = 0;
+    for (; i + U <= ncols; i += U) {
+      VT v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) v[u] = __ldcs(reinterpret_cast<const VT*>(V + (size_t)(i + u) * ld) + vi);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const double ci = cs_[i + u];
+#pragma unroll
+        for (int e = 0; e < N; ++e) x[e] -= ci * Vec4<T>::get(v[u], e);
+      }
+    }
+    for (; i < ncols; ++i) {
       const VT v = __ldcs(reinterpret_cast<const VT*>(V + (size_t)i * ld) + vi);
       const double ci = cs_[i];
 #pragma unroll
