@@ -705,8 +705,11 @@ def main():
                                         "format": ("cell-block (bs %d)" % fb if fb else "CSR")
                                         + (", %d/%d padded slots" % Fg.padded if Fg.padded[0] else ""),
                                         "note": "the intermediate FL x (64 MB) stays in L2 between the two products"}
+    plans = {"A_f64": A.product_plan(64)}
     del P64
-    P32 = d.CPR(PREC, d.CSR(n, n, r_d, c_d, v_d, ctx), b_d.clone(), precision=32)
+    A32 = d.CSR(n, n, r_d, c_d, v_d, ctx)
+    P32 = d.CPR(PREC, A32, b_d.clone(), precision=32)
+    plans["A_f32"] = A32.product_plan(32)
     Fg32 = P32.fsai(0)
     fb, kl, ku = Fg32.blocks
     # as the mixed-precision CPR applies it: float32 x, intermediate and y
@@ -721,7 +724,7 @@ def main():
     kernels["fsai_apply_global_f32_f64io"] = {"ms": ms, "gbs": algF32d / ms / 1e6, "alg_bytes": algF32d,
                                               "format": "cell-block (bs %d)" % fb if fb else "CSR",
                                               "vectors": "float64 (deco_fsai_apply)"}
-    del P32, A, b, x64, y64, x32, y32
+    del P32, A32, A, b, x64, y64, x32, y32
     # the orthogonalisation (dot pass + update pass of every Arnoldi step), timed by CUDA
     # events around each step's phases inside one mixed solve (DECO_PROFILE=1).  Bytes of
     # step j with a float32 basis: 2 (j + 3) 4n (each pass reads the j + 1 columns and w;
@@ -808,6 +811,8 @@ def main():
         "gpu_launches": launches,
         "roofline": roofline,
         "kernels": kernels,
+        # the product the CPR setup's autotuner chose for A: (padded | cells | csr, lanes per cell or row)
+        "product_plans": plans,
         "cpu_baseline": cpu,
         "e2e": e2e,
         "clocks": clocks,

@@ -201,6 +201,14 @@ class CSR:
         check(lib().deco_csr_padded(self.h, C.byref(w)))
         return w.value
 
+    def product_plan(self, precision: int = 64):
+        """(kind, lanes) of the product y = A x takes: kind "padded" (rows grouped per
+        thread), "cells" (lanes per cell) or "csr" (lanes per row), as the
+        autotuner of a CPR setup chose it, or the layout rules."""
+        k, w = C.c_int(), C.c_int()
+        check(lib().deco_csr_product_plan(self.h, precision, C.byref(k), C.byref(w)))
+        return {1: "padded", 2: "cells", 3: "csr"}[k.value], w.value
+
     def transpose(self) -> "CSR":
         """A^T on the device, rows in ascending column order."""
         h = C.c_void_p()

@@ -65,6 +65,7 @@ SIGNATURES = {
     "deco_csr_set_blocks": ([vp, vp, C.c_int], C.c_int),
     "deco_csr_blocks": ([vp, ip, ip], C.c_int),
     "deco_csr_padded": ([vp, ip], C.c_int),
+    "deco_csr_product_plan": ([vp, C.c_int, ip, ip], C.c_int),
     "deco_spmv": ([vp, vp, vp, vp, C.c_int], C.c_int),
     "deco_spmv_f32": ([vp, vp, vp, vp, C.c_int], C.c_int),
     "deco_residual": ([vp, vp, vp, vp, vp], C.c_int),

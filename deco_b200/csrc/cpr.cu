@@ -572,6 +572,12 @@ static void cpr_build(deco_ctx_s* ctx, deco_csr_s* A, double* d_b, const deco_cp
       tuned_bsr_subwarp(ctx, M, false);
       if (prm.precision == 32) tuned_bsr_subwarp(ctx, M, true);
     }
+  // then which product each matrix takes (slot-padded, cell blocks or CSR)
+  for (deco_csr_s* M : {A, &P->glo.FL, &P->glo.FUt, &P->loc.FL, &P->loc.FUt})
+    if (M->n) {
+      tune_product_plan(ctx, M, false);
+      if (prm.precision == 32) tune_product_plan(ctx, M, true);
+    }
   DECO_CUDA(cudaStreamSynchronize(st));
   P->t_ms[4] = P->t_ms[0] + P->t_ms[1] + P->t_ms[2] + P->t_ms[3] + ev.stop();
 }

@@ -298,6 +298,74 @@ int tuned_bsr_subwarp(deco_ctx_s* ctx, deco_csr_s* A, bool f32) {
   return sw;
 }
 
+void tune_product_plan(deco_ctx_s* ctx, deco_csr_s* A, bool f32) {
+  int& plan = f32 ? A->plan32 : A->plan64;
+  if (plan || !ctx->autotune || A->n < 4096 || (f32 && !A->v32)) return;
+  const bool ell = A->ew && (!f32 || A->ev32) && (A->bbs == 2 || A->bbs == 0);
+  const bool cells = A->bbs > 1 && (!f32 || A->bv32);
+  const int first = ell ? 1 : (cells ? 2 : 3);  // what the layout rules pick
+  if (!ell && !cells) return;                    // CSR is the only product
+  static std::map<std::tuple<int, int, int, int, int, bool>, int> cache;
+  static std::mutex mu;
+  const auto key = std::make_tuple(A->n, A->m, A->nz, A->bbs, A->ew, f32);
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) { plan = it->second; return; }
+  }
+  cudaStreamCaptureStatus cs;
+  DECO_CUDA(cudaStreamIsCapturing(ctx->stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return;
+  // the candidates' own widths first (they time themselves once)
+  const int csw = tuned_subwarp(ctx, A, f32);
+  const int bsw = cells ? tuned_bsr_subwarp(ctx, A, f32) : 0;
+  DevBuf<double> x(A->m, ctx->stream), y(A->n, ctx->stream);
+  DevBuf<float> xf, yf;
+  x.zero(ctx->stream);
+  if (f32) { xf.alloc(A->m, ctx->stream); yf.alloc(A->n, ctx->stream); xf.zero(ctx->stream); }
+  auto run = [&](int cand) {
+    if (f32) {
+      if (cand == 1 && A->bbs) launch_ell2<float, float>(ctx->stream, A, false, xf.get(), EpiStore<float>{yf.get()});
+      else if (cand == 1) launch_ell1<float, float>(ctx->stream, A, xf.get(), EpiStore<float>{yf.get()});
+      else if (cand == 2) launch_bsr<float, float>(ctx->stream, A, bsw, false, xf.get(), EpiStore<float>{yf.get()});
+      else launch_spmv_sw<float, float>(ctx->stream, csw, A->n, 1, A->r.get(), A->c.get(), A->v32.get(), xf.get(),
+                                          EpiStore<float>{yf.get()});
+    } else {
+      if (cand == 1 && A->bbs) launch_ell2<double, double>(ctx->stream, A, false, x.get(), EpiStore<double>{y.get()});
+      else if (cand == 1) launch_ell1<double, double>(ctx->stream, A, x.get(), EpiStore<double>{y.get()});
+      else if (cand == 2) launch_bsr<double, double>(ctx->stream, A, bsw, false, x.get(), EpiStore<double>{y.get()});
+      else launch_spmv_sw<double, double>(ctx->stream, csw, A->n, 1, A->r.get(), A->c.get(), A->v.get(), x.get(),
+                                            EpiStore<double>{y.get()});
+    }
+  };
+  auto time_plan = [&](int cand) {
+    float t[5];
+    for (int rep = 0; rep < 6; ++rep) {
+      DECO_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+      run(cand);
+      DECO_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+      DECO_CUDA(cudaEventSynchronize(ctx->ev1));
+      float ms = 0.f;
+      DECO_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+      if (rep > 0) t[rep - 1] = ms;
+    }
+    std::sort(t, t + 5);
+    return t[2];
+  };
+  const float t_first = time_plan(first);
+  float best = t_first;
+  int choice = first;
+  for (int cand = first + 1; cand <= 3; ++cand) {
+    if (cand == 2 && !cells) continue;
+    const float tc = time_plan(cand);
+    if (tc < best) { best = tc; choice = cand; }
+  }
+  if (best > 0.95f * t_first) choice = first;
+  plan = choice;
+  std::lock_guard<std::mutex> lk(mu);
+  cache[key] = plan;
+}
+
 int tuned_subwarp(deco_ctx_s* ctx, deco_csr_s* A, bool f32) {
   int& sw = f32 ? A->sw32 : A->sw64;
   if (sw) return sw;
@@ -466,6 +534,22 @@ int deco_csr_padded(deco_csr A, int* slots) {
   return guard([&] {
     DECO_REQUIRE(A && slots, DECO_ERR_ARG, "NULL argument");
     *slots = A->ew;
+  });
+}
+
+int deco_csr_product_plan(deco_csr A, int precision, int* kind, int* lanes) {
+  return guard([&] {
+    DECO_REQUIRE(A && kind && lanes, DECO_ERR_ARG, "NULL argument");
+    DECO_REQUIRE(precision == 64 || precision == 32, DECO_ERR_ARG, "precision must be 64 or 32");
+    const bool f32 = precision == 32;
+    const int plan = f32 ? A->plan32 : A->plan64;
+    const bool cells = A->bbs > 1 && (!f32 || A->bv32);
+    const bool ell = A->ew && (!f32 || A->ev32);
+    int k = 3;  // the dispatch of spmv() for a full product with aligned x
+    if (plan != 3 && cells) k = (plan != 2 && ell) ? 1 : 2;
+    else if (plan != 3 && !A->bbs && ell) k = 1;
+    *kind = k;
+    *lanes = k == 1 ? 1 : (k == 2 ? (f32 ? A->bsw32 : A->bsw64) : (f32 ? A->sw32 : A->sw64));
   });
 }
 

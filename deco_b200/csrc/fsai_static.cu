@@ -23,12 +23,11 @@
 //     needs clearing, since the first product writes every entry before the
 //     second reads it;
 //   * calls that overlap on the GPU (two streams at once) race on the array;
-//   * the two products use the kernels deco_fsai_apply uses whenever those need no
-//     allocation (the slot-padded copies), so the results are identical to its
-//     results then; a factor without padded copies goes through the CSR kernel
-//     at the heuristic width (no timing, no shared state), which sums in another
-//     order than the cell-block kernel deco_fsai_apply may pick: equal to
-//     rounding, not bit for bit.
+//   * the two products take the product deco_fsai_apply takes (the autotuner's
+//     choice, or the layout rules): with the slot-padded copies the results are
+//     identical to its results; the cell-block and CSR kernels run at their
+//     heuristic widths here (no timing, no shared state), which may sum in
+//     another order than deco_fsai_apply's tuned widths: equal to rounding.
 #include <map>
 #include <mutex>
 
@@ -74,7 +73,15 @@ int width_no_alloc(const deco_csr_s* A, bool f32) { return heuristic_subwarp(A->
 template <typename VT, typename XT, class Epi>
 void product_no_alloc(deco_ctx_s* ctx, deco_csr_s* A, const XT* x, Epi epi) {
   const bool f32 = sizeof(VT) == 4;
-  if (A->ew && (!f32 || A->ev32)) {
+  const int plan = f32 ? A->plan32 : A->plan64;  // the product autotuner's choice (0: the layout rules)
+  if (plan == 2 && A->bbs > 1 && (!f32 || A->bv32) &&
+      reinterpret_cast<uintptr_t>(x) % (A->bbs == 2 ? 2 * sizeof(XT) : sizeof(XT)) == 0) {
+    int sw = 1;  // the cell-block kernel's heuristic lanes per cell (no shared state)
+    while (sw < 16 && sw < A->avg_blk / (A->bbs == 2 ? 4.0 : 2.0)) sw <<= 1;
+    launch_bsr<VT, XT, Epi>(ctx->stream, A, sw, false, x, epi);
+    return;
+  }
+  if (plan != 3 && A->ew && (!f32 || A->ev32)) {
     if (!A->bbs) {
       launch_ell1<VT, XT, Epi>(ctx->stream, A, x, epi);
       return;

@@ -53,6 +53,10 @@ struct deco_csr_s {
   deco::DevBuf<int> ec;
   deco::DevBuf<double> ev;
   deco::DevBuf<float> ev32;
+  // The product the autotuner chose per value precision (tune_product_plan):
+  // 0 = not chosen (the layout rules: slot-padded copy, else cell blocks, else
+  // CSR), 1 = slot-padded copy, 2 = cell-block kernel, 3 = CSR kernel.
+  int plan64 = 0, plan32 = 0;
 };
 
 namespace deco {
@@ -528,6 +532,15 @@ int tuned_subwarp(deco_ctx_s* ctx, deco_csr_s* A, bool f32);
 // tuned_subwarp.
 int tuned_bsr_subwarp(deco_ctx_s* ctx, deco_csr_s* A, bool f32);
 
+// The product autotuner: times every product A has a layout for -- the
+// slot-padded copy (a thread per cell or per row: rows grouped per thread), the
+// cell-block kernel at its tuned lanes per cell, the CSR kernel at its tuned
+// lanes per row -- once per matrix shape and value precision (cached across
+// setups), and records the fastest in A->plan64 / plan32, keeping the layout
+// rules' choice unless another is at least 5 % faster.  No-op without
+// ctx->autotune, below 4096 rows, or inside a stream capture.
+void tune_product_plan(deco_ctx_s* ctx, deco_csr_s* A, bool f32);
+
 // Builds (or rebuilds) the cell-block copy of A for bs x bs cells when the
 // zero padding stays within max_fill x nz stored values; otherwise A keeps no
 // block copy.  Float32 planes are made when A has float32 values.
@@ -550,16 +563,17 @@ void drop_bsr(deco_csr_s* A);
 template <typename VT, typename XT, class Epi>
 void spmv(deco_ctx_s* ctx, deco_csr_s* A, const XT* x, Epi epi, int bs = 1) {
   const bool f32 = sizeof(VT) == 4;
-  if (A->bbs > 1 && (bs == 1 || bs == A->bbs) && (!f32 || A->bv32) &&
+  const int plan = f32 ? A->plan32 : A->plan64;  // 0: the layout rules below
+  if (plan != 3 && A->bbs > 1 && (bs == 1 || bs == A->bbs) && (!f32 || A->bv32) &&
       (reinterpret_cast<uintptr_t>(x) % (A->bbs == 2 ? 2 * sizeof(XT) : sizeof(XT))) == 0) {
-    if (A->ew && (!f32 || A->ev32)) {
+    if (plan != 2 && A->ew && (!f32 || A->ev32)) {
       launch_ell2<VT, XT, Epi>(ctx->stream, A, bs != 1, x, epi);
       return;
     }
     launch_bsr<VT, XT, Epi>(ctx->stream, A, tuned_bsr_subwarp(ctx, A, f32), bs != 1, x, epi);
     return;
   }
-  if (!A->bbs && A->ew && bs == 1 && (!f32 || A->ev32)) {
+  if (plan != 3 && !A->bbs && A->ew && bs == 1 && (!f32 || A->ev32)) {
     launch_ell1<VT, XT, Epi>(ctx->stream, A, x, epi);
     return;
   }

@@ -110,6 +110,15 @@ int deco_csr_blocks(deco_csr A, int* bs, int* nblk);
  * made with the block copy; DECO_PADDED=0 in the environment at context
  * creation turns both off.  No counterpart in the reference. */
 int deco_csr_padded(deco_csr A, int* slots);
+/* The product a full y = A x of this matrix takes for float64 (precision 64) or
+ * float32 (32) values: kind 1 = the slot-padded copy (one thread per cell of
+ * 2x2 blocks, or per scalar row: rows grouped per thread), 2 = the cell-block
+ * kernel with `lanes` lanes per cell, 3 = the CSR kernel with `lanes` lanes per
+ * row.  A CPR setup times the products each of its matrices has a layout for
+ * and keeps the fastest (the layout rules' choice unless another is at least
+ * 5 % faster; DECO_AUTOTUNE=0 keeps the rules).  No counterpart in the
+ * reference. */
+int deco_csr_product_plan(deco_csr A, int precision, int* kind, int* lanes);
 
 /* y = A x (bs == 1), or the restricted product of alg::spmv with bs > 1:
  * y[i/bs] = (A x)[i] for rows i = 0, bs, 2bs, ...   (core/alg.hpp:50-64,

@@ -143,3 +143,24 @@ def test_cpr_builds_blocks_and_keeps_parity(d, precision):
     S = d.SOL(sol_json(), A, P, b, precision=precision)
     ref_it = O.solve(sol_json())["iter"]
     assert S.flag == 0 and abs(S.iter - ref_it) <= max(2, 0.1 * ref_it)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_product_plan_chosen_by_the_cpr_autotuner(d, precision):
+    """A CPR setup times the products each of its matrices has a layout for (slot-padded
+    copy, cell-block kernel, CSR kernel) and keeps the fastest; the chosen product of A
+    is reported, and the CPR apply through it still matches the oracle."""
+    from conftest import cpr_json
+    from oracle import port
+    s = gen.generate(gen.preset(1))
+    A = d.CSR.from_system(s)
+    b = torch.from_numpy(s.b.copy()).cuda()
+    P = d.CPR(cpr_json(2), A, b, precision=precision)
+    kind, lanes = A.product_plan(precision)
+    assert kind in ("padded", "cells", "csr") and lanes >= 1
+    if precision == 64:
+        O = port.Cpr(cpr_json(2), s.r, s.c, s.v, s.b)
+        rv = np.random.default_rng(9).standard_normal(s.n)
+        x = P.apply(torch.from_numpy(rv).cuda()).cpu().numpy()
+        xo = O.apply(rv)
+        assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-12
