@@ -680,27 +680,31 @@ def main():
     nzF = Fg.nz
     kernels = {}
 
-    def matrix_bytes(nz, blocks, vb):
+    def matrix_bytes(nz, blocks, vb, ib=4):
         """Bytes of one pass over a matrix in the layout the product reads: the
-        cell-block copy (one 4-byte index per bs x bs block, block-row pointers)
-        when there is one, else CSR (4-byte index + value per entry)."""
+        cell-block copy (one column index of ib bytes per bs x bs block -- 4, or the
+        1- or 2-byte offset code of the padded copy -- and block-row pointers) when
+        there is one, else CSR (4-byte index + value per entry)."""
         bsz, nblk = blocks
         if bsz:
-            return nblk * 4 + nblk * bsz * bsz * vb + 4 * (n // bsz + 1)
+            return nblk * ib + nblk * bsz * bsz * vb + 4 * (n // bsz + 1)
         return nz * (4 + vb) + 4 * (n + 1)
 
+    cb = A.slot_codes[0] if A.padded else 4  # bytes per block column the padded product reads
     fmt = ("cell-block (bs %d)" % A.blocks[0] if A.blocks[0] else "CSR") + \
-        (", %d padded slots per cell" % A.padded if A.padded else "")
+        (", %d padded slots per cell" % A.padded if A.padded else "") + \
+        (", %d-byte column offset codes" % cb if A.padded and cb < 4 else "")
     ms = kernel_ms(lambda: A.apply_f32(x32, y32))
-    alg32 = matrix_bytes(nnz, A.blocks, 4) + 4 * n + 4 * n
+    alg32 = matrix_bytes(nnz, A.blocks, 4, cb) + 4 * n + 4 * n
     kernels["spmv_A_f32"] = {"ms": ms, "gbs": alg32 / ms / 1e6, "alg_bytes": alg32, "format": fmt,
                              "subwarp": A.subwarp}
     ms = kernel_ms(lambda: A.apply(x64, y64))
-    alg64 = matrix_bytes(nnz, A.blocks, 8) + 8 * n + 8 * n
+    alg64 = matrix_bytes(nnz, A.blocks, 8, cb) + 8 * n + 8 * n
     kernels["spmv_A_f64"] = {"ms": ms, "gbs": alg64 / ms / 1e6, "alg_bytes": alg64, "format": fmt}
     fb, kl, ku = Fg.blocks
     ms = kernel_ms(lambda: Fg.apply(x64, y64))
-    algF = matrix_bytes(nzF, (fb, kl), 8) + matrix_bytes(nzF, (fb, ku), 8) + 8 * n + 2 * 8 * n + 8 * n
+    cl, cu = (b_ if b_ else 4 for b_ in Fg.slot_codes)
+    algF = matrix_bytes(nzF, (fb, kl), 8, cl) + matrix_bytes(nzF, (fb, ku), 8, cu) + 8 * n + 2 * 8 * n + 8 * n
     kernels["fsai_apply_global_f64"] = {"ms": ms, "gbs": algF / ms / 1e6, "alg_bytes": algF, "nnz_factor": nzF,
                                         "format": ("cell-block (bs %d)" % fb if fb else "CSR")
                                         + (", %d/%d padded slots" % Fg.padded if Fg.padded[0] else ""),
@@ -714,13 +718,14 @@ def main():
     fb, kl, ku = Fg32.blocks
     # as the mixed-precision CPR applies it: float32 x, intermediate and y
     ms = kernel_ms(lambda: Fg32.apply_f32(x32, y32))
-    algF32 = matrix_bytes(nzF, (fb, kl), 4) + matrix_bytes(nzF, (fb, ku), 4) + 4 * n + 2 * 4 * n + 4 * n
+    cl, cu = (b_ if b_ else 4 for b_ in Fg32.slot_codes)
+    algF32 = matrix_bytes(nzF, (fb, kl), 4, cl) + matrix_bytes(nzF, (fb, ku), 4, cu) + 4 * n + 2 * 4 * n + 4 * n
     kernels["fsai_apply_global_f32"] = {"ms": ms, "gbs": algF32 / ms / 1e6, "alg_bytes": algF32,
                                         "format": "cell-block (bs %d)" % fb if fb else "CSR",
                                         "vectors": "float32 (deco_fsai_apply_f32)"}
     # through the reference-shaped interface: float64 x and y around the float32 factor
     ms = kernel_ms(lambda: Fg32.apply(x64, y64))
-    algF32d = matrix_bytes(nzF, (fb, kl), 4) + matrix_bytes(nzF, (fb, ku), 4) + 8 * n + 2 * 4 * n + 8 * n
+    algF32d = matrix_bytes(nzF, (fb, kl), 4, cl) + matrix_bytes(nzF, (fb, ku), 4, cu) + 8 * n + 2 * 4 * n + 8 * n
     kernels["fsai_apply_global_f32_f64io"] = {"ms": ms, "gbs": algF32d / ms / 1e6, "alg_bytes": algF32d,
                                               "format": "cell-block (bs %d)" % fb if fb else "CSR",
                                               "vectors": "float64 (deco_fsai_apply)"}
@@ -759,7 +764,9 @@ def main():
                 "kernel": ("deco::%s (2x2 cell blocks, padded slots per cell)" % kname if kname else
                            "deco::bsr2_pair_kernel / bsr_kernel / spmv_kernel (float32)")
                 + " on A (%d rows, %d nnz, float32 values)" % (n, nnz),
-                "algorithmic_bytes": "the unpadded cell-block layout's bytes (padding slots count against the kernel)",
+                "algorithmic_bytes": "the unpadded cell-block layout's bytes, block columns in the padded copy's "
+                                     "encoding (1-byte offset codes when it has them); padding slots count against "
+                                     "the kernel",
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind}
 
     rec3 = reference_record(CONFIG) if GRID is None else None

@@ -209,6 +209,14 @@ class CSR:
         check(lib().deco_csr_product_plan(self.h, precision, C.byref(k), C.byref(w)))
         return {1: "padded", 2: "cells", 3: "csr"}[k.value], w.value
 
+    @property
+    def slot_codes(self):
+        """(bytes per slot column the padded products read: 1, 2 or 4, 0 without a
+        padded copy; distinct column offsets the codes select)."""
+        b, k = C.c_int(), C.c_int()
+        check(lib().deco_csr_slot_codes(self.h, C.byref(b), C.byref(k)))
+        return b.value, k.value
+
     def transpose(self) -> "CSR":
         """A^T on the device, rows in ascending column order."""
         h = C.c_void_p()
@@ -286,6 +294,13 @@ class FSAI:
         """(slots of FL's, slots of FU^T's) padded copies (4, 7 or 8; 0 without)."""
         a, b = C.c_int(), C.c_int()
         check(lib().deco_fsai_padded(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    @property
+    def slot_codes(self):
+        """Bytes per slot column of FL's and FU^T's padded copies (1, 2 or 4; 0 without)."""
+        a, b = C.c_int(), C.c_int()
+        check(lib().deco_fsai_slot_codes(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
 
     @property

@@ -66,6 +66,7 @@ SIGNATURES = {
     "deco_csr_blocks": ([vp, ip, ip], C.c_int),
     "deco_csr_padded": ([vp, ip], C.c_int),
     "deco_csr_product_plan": ([vp, C.c_int, ip, ip], C.c_int),
+    "deco_csr_slot_codes": ([vp, ip, ip], C.c_int),
     "deco_spmv": ([vp, vp, vp, vp, C.c_int], C.c_int),
     "deco_spmv_f32": ([vp, vp, vp, vp, C.c_int], C.c_int),
     "deco_residual": ([vp, vp, vp, vp, vp], C.c_int),
@@ -76,6 +77,7 @@ SIGNATURES = {
     "deco_fsai_download": ([vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
     "deco_fsai_apply": ([vp, vp, vp, vp], C.c_int),
     "deco_fsai_padded": ([vp, ip, ip], C.c_int),
+    "deco_fsai_slot_codes": ([vp, ip, ip], C.c_int),
     "deco_fsai_apply_f32": ([vp, vp, vp, vp], C.c_int),
     "deco_fsai_apply_static": ([vp, vp, vp, vp], C.c_int),
     "deco_cpr_create": ([vp, vp, vp, C.POINTER(CprParams), C.POINTER(vp)], C.c_int),

@@ -144,6 +144,7 @@ struct deco_ctx_s {
   int autotune = 1;
   int bsr = 1;        // cell-block copies for CPR systems (DECO_BSR=0 disables)
   int padded = 1;     // slot-padded copies of short-row 2x2-block matrices (DECO_PADDED=0 disables)
+  int slot_codes = 1; // offset-coded slot columns of the padded copies (DECO_SLOT_CODES=0 disables)
   int trace = 0;      // DECO_TRACE=1: host wall time of setup sub-steps on stderr
   double trace_t = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;

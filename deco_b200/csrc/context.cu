@@ -279,6 +279,7 @@ int deco_ctx_create(int device, void* stream, deco_ctx* out) {
     if (const char* e = std::getenv("DECO_AUTOTUNE")) c->autotune = std::atoi(e) != 0;
     if (const char* e = std::getenv("DECO_BSR")) c->bsr = std::atoi(e) != 0;
     if (const char* e = std::getenv("DECO_PADDED")) c->padded = std::atoi(e) != 0;
+    if (const char* e = std::getenv("DECO_SLOT_CODES")) c->slot_codes = std::atoi(e) != 0;
     if (const char* e = std::getenv("DECO_TRACE")) c->trace = std::atoi(e) != 0;
     // keep freed device memory in the stream-ordered pool instead of returning it
     cudaMemPool_t pool;

@@ -5,6 +5,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <vector>
 
 #include "spmv.cuh"
 
@@ -88,6 +89,102 @@ __global__ void ell2_fill(int nbr, int W, const int* __restrict__ br, const int*
   }
 }
 
+// ---- offset-coded slot columns
+// The distinct column offsets of the slots (column minus the slot's own row or
+// cell) go into an open-addressing set of kSetCap entries; when more than
+// kMaxCodes distinct offsets appear the set stops growing and the count says so.
+constexpr int kSetCap = 1 << 17;
+constexpr int kMaxCodes = 1 << 16;
+constexpr int kSetEmpty = (int)0x80808080u;  // what a 0x80 byte fill leaves (no offset of an int32-indexed matrix reaches it)
+
+__global__ void slot_offset_set(long long total, int nrow, const int* __restrict__ ec, int* __restrict__ set,
+                                int* __restrict__ count) {
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int d = ec[idx] - (int)(idx % nrow);
+    // one lane per distinct offset of the warp inserts (neighbouring rows mostly share them)
+    const unsigned same = __match_any_sync(__activemask(), d);
+    if ((threadIdx.x & 31) != __ffs(same) - 1) continue;
+    unsigned h = ((unsigned)d * 2654435761u) & (kSetCap - 1);
+    for (int probe = 0; probe < kSetCap; ++probe) {
+      const int cur = __ldcg(set + h);
+      if (cur == d) break;
+      if (cur == kSetEmpty) {
+        if (*(volatile int*)count > kMaxCodes) break;  // too many: the matrix keeps 4-byte columns
+        const int prev = atomicCAS(set + h, kSetEmpty, d);
+        if (prev == kSetEmpty) { atomicAdd(count, 1); break; }
+        if (prev == d) break;
+      }
+      h = (h + 1) & (kSetCap - 1);
+    }
+  }
+}
+
+// the set's entries into packed[0..count) (nothing when the set overflowed)
+__global__ void slot_offset_pack(const int* __restrict__ set, const int* __restrict__ count, int* __restrict__ packed,
+                                 int* __restrict__ npacked) {
+  if (*count > kMaxCodes) return;
+  for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < kSetCap; h += gridDim.x * blockDim.x) {
+    const int d = set[h];
+    if (d != kSetEmpty) packed[atomicAdd(npacked, 1)] = d;
+  }
+}
+
+template <typename CT>
+__global__ void slot_codes(long long total, int nrow, const int* __restrict__ ec, const int* __restrict__ off,
+                           int noff, CT* __restrict__ code) {
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int d = ec[idx] - (int)(idx % nrow);
+    int lo = 0, hi = noff - 1;  // off is sorted and holds d
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(off + mid) < d) lo = mid + 1; else hi = mid;
+    }
+    code[idx] = (CT)lo;
+  }
+}
+
+void make_slot_codes(deco_ctx_s* ctx, deco_csr_s* A, int nrow) {
+  A->eb = A->noff = 0;
+  A->ecode = DevBuf<unsigned char>();
+  A->eoff = DevBuf<int>();
+  if (!ctx->slot_codes || !A->ew || nrow <= 0 || !A->ec) return;
+  cudaStream_t st = ctx->stream;
+  const long long total = (long long)A->ew * nrow;
+  DevBuf<int> set(kSetCap, st), count(1, st);
+  DECO_CUDA(cudaMemsetAsync(set.get(), 0x80, sizeof(int) * kSetCap, st));  // every entry kSetEmpty
+  count.zero(st);
+  const int g = grid_for(ctx, total, 256);
+  slot_offset_set<<<g, 256, 0, st>>>(total, nrow, A->ec.get(), set.get(), count.get());
+  DECO_CHECK_LAUNCH();
+  // the set's entries, compacted on the device (only they travel to the host)
+  DevBuf<int> packed(kMaxCodes + 64, st), npacked(1, st);
+  npacked.zero(st);
+  slot_offset_pack<<<grid_for(ctx, kSetCap, 256), 256, 0, st>>>(set.get(), count.get(), packed.get(), npacked.get());
+  DECO_CHECK_LAUNCH();
+  int nd = 0;
+  DECO_CUDA(cudaMemcpyAsync(&nd, count.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+  DECO_CUDA(cudaStreamSynchronize(st));
+  if (nd <= 0 || nd > kMaxCodes) return;
+  std::vector<int> off(nd);
+  DECO_CUDA(cudaMemcpyAsync(off.data(), packed.get(), sizeof(int) * nd, cudaMemcpyDeviceToHost, st));
+  DECO_CUDA(cudaStreamSynchronize(st));
+  std::sort(off.begin(), off.end());
+  A->eoff.alloc(off.size(), st);
+  DECO_CUDA(cudaMemcpyAsync(A->eoff.get(), off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, st));
+  A->noff = nd;
+  A->eb = nd <= 256 ? 1 : 2;
+  A->ecode.alloc((size_t)total * A->eb, st);
+  if (A->eb == 1)
+    slot_codes<unsigned char><<<g, 256, 0, st>>>(total, nrow, A->ec.get(), A->eoff.get(), nd, A->ecode.get());
+  else
+    slot_codes<unsigned short><<<g, 256, 0, st>>>(total, nrow, A->ec.get(), A->eoff.get(), nd,
+                                                   reinterpret_cast<unsigned short*>(A->ecode.get()));
+  DECO_CHECK_LAUNCH();
+  DECO_CUDA(cudaStreamSynchronize(st));  // `off` (host) must outlive the copy
+}
+
 void make_padded(deco_ctx_s* ctx, deco_csr_s* A) {
   cudaStream_t st = ctx->stream;
   const int nbr = A->n / 2;
@@ -111,6 +208,7 @@ void make_padded(deco_ctx_s* ctx, deco_csr_s* A) {
     ell2_fill<double><<<grid_for(ctx, nbr, 256), 256, 0, st>>>(nbr, W, A->br.get(), A->bc.get(), A->bv.get(),
                                                                A->bplane, A->ec.get(), A->ev.get());
     DECO_CHECK_LAUNCH();
+    make_slot_codes(ctx, A, nbr);
   }
   if (A->bv32) {
     const int W = A->ew;
@@ -151,6 +249,7 @@ void make_padded_scalar(deco_ctx_s* ctx, deco_csr_s* A) {
     ell1_fill<double><<<grid_for(ctx, n, 256), 256, 0, st>>>(n, W, A->r.get(), A->c.get(), A->v.get(), A->ec.get(),
                                                               A->ev.get());
     DECO_CHECK_LAUNCH();
+    make_slot_codes(ctx, A, n);
   }
   if (A->v32) {
     const int W = A->ew;
@@ -174,6 +273,9 @@ void drop_bsr(deco_csr_s* A) {
   A->ec = DevBuf<int>();
   A->ev = DevBuf<double>();
   A->ev32 = DevBuf<float>();
+  A->eb = A->noff = 0;
+  A->ecode = DevBuf<unsigned char>();
+  A->eoff = DevBuf<int>();
 }
 
 void make_bsr(deco_ctx_s* ctx, deco_csr_s* A, int bs, double max_fill) {
@@ -223,6 +325,9 @@ void refresh_stats(deco_ctx_s* ctx, deco_csr_s* A) {
     A->ec = DevBuf<int>();
     A->ev = DevBuf<double>();
     A->ev32 = DevBuf<float>();
+    A->eb = A->noff = 0;
+    A->ecode = DevBuf<unsigned char>();
+    A->eoff = DevBuf<int>();
   }
 }
 
@@ -550,6 +655,14 @@ int deco_csr_product_plan(deco_csr A, int precision, int* kind, int* lanes) {
     else if (plan != 3 && !A->bbs && ell) k = 1;
     *kind = k;
     *lanes = k == 1 ? 1 : (k == 2 ? (f32 ? A->bsw32 : A->bsw64) : (f32 ? A->sw32 : A->sw64));
+  });
+}
+
+int deco_csr_slot_codes(deco_csr A, int* bytes, int* noffsets) {
+  return guard([&] {
+    DECO_REQUIRE(A && bytes && noffsets, DECO_ERR_ARG, "NULL argument");
+    *bytes = !A->ew ? 0 : (A->eb ? A->eb : 4);
+    *noffsets = A->noff;
   });
 }
 

@@ -776,6 +776,14 @@ int deco_fsai_padded(deco_fsai F, int* slots_lower, int* slots_upper) {
   });
 }
 
+int deco_fsai_slot_codes(deco_fsai F, int* bytes_lower, int* bytes_upper) {
+  return guard([&] {
+    DECO_REQUIRE(F, DECO_ERR_ARG, "F is NULL");
+    if (bytes_lower) *bytes_lower = !F->FL.ew ? 0 : (F->FL.eb ? F->FL.eb : 4);
+    if (bytes_upper) *bytes_upper = !F->FUt.ew ? 0 : (F->FUt.eb ? F->FUt.eb : 4);
+  });
+}
+
 int deco_fsai_download(deco_ctx ctx, deco_fsai F, int* Lr, int* Lc, double* Lv, int* Ur, int* Uc, double* Uv) {
   int rc = deco_csr_download(ctx, &F->FL, Lr, Lc, Lv);
   if (rc) return rc;

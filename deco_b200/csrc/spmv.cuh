@@ -53,6 +53,15 @@ struct deco_csr_s {
   deco::DevBuf<int> ec;
   deco::DevBuf<double> ev;
   deco::DevBuf<float> ev32;
+  // Offset-coded slot columns: when the slots' column offsets (block column
+  // minus the cell's own index, or column minus the row for scalar rows) take at
+  // most 256 (eb = 1) or 65536 (eb = 2) distinct values, eoff holds them sorted
+  // and ecode[k * nrow + s] (eb bytes each) the position of slot k's offset, so
+  // the products read 1 or 2 bytes per slot instead of a 4-byte column.  eb = 0:
+  // the products read ec.
+  int eb = 0, noff = 0;
+  deco::DevBuf<unsigned char> ecode;
+  deco::DevBuf<int> eoff;
   // The product the autotuner chose per value precision (tune_product_plan):
   // 0 = not chosen (the layout rules: slot-padded copy, else cell blocks, else
   // CSR), 1 = slot-padded copy, 2 = cell-block kernel, 3 = CSR kernel.
@@ -368,9 +377,21 @@ __global__ void __launch_bounds__(256) bsr2_pair_kernel(int nbr, const int* __re
 // slot order, i.e. the cell's block order.  (Measured on B200 for the lower FSAI
 // factor of the 8M-row system, four blocks per cell, L2 flushed: 65 us float32 and
 // 111 us float64, against 89 us and 152 us with the pair kernel.)
-template <int W, bool ROW0, typename VT, typename XT, class Epi>
+// Column of slot entry idx of the padded copy whose own row (or cell) is `base`:
+// the stored column (EB = 0), or base + the offset the 1- or 2-byte code selects.
+template <int EB>
+__device__ __forceinline__ int slot_col(const int* __restrict__ ec, const unsigned char* __restrict__ code,
+                                        const int* __restrict__ off, long long idx, int base) {
+  if constexpr (EB == 0) return __ldcs(ec + idx);
+  else if constexpr (EB == 1) return base + __ldg(off + __ldcs(code + idx));
+  else return base + __ldg(off + __ldcs(reinterpret_cast<const unsigned short*>(code) + idx));
+}
+
+template <int W, bool ROW0, typename VT, typename XT, class Epi, int EB = 0>
 __global__ void __launch_bounds__(256) ell2_kernel(int nbr, const int* __restrict__ ec, const VT* __restrict__ ev,
-                                                   const XT* __restrict__ x, Epi epi) {
+                                                   const XT* __restrict__ x, Epi epi,
+                                                   const unsigned char* __restrict__ code = nullptr,
+                                                   const int* __restrict__ off = nullptr) {
   using V2 = typename Pair<VT>::V;
   using X2 = typename Pair<XT>::V;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -380,7 +401,7 @@ __global__ void __launch_bounds__(256) ell2_kernel(int nbr, const int* __restric
   V2 a[W], b[W];
 #pragma unroll
   for (int k = 0; k < W; ++k) {
-    cc[k] = __ldcs(ec + (long long)k * nbr + s);
+    cc[k] = slot_col<EB>(ec, code, off, (long long)k * nbr + s, s);
     a[k] = __ldcs(e2 + (long long)k * nbr + s);
     if (!ROW0) b[k] = __ldcs(e2 + (long long)(W + k) * nbr + s);
   }
@@ -412,16 +433,18 @@ __global__ void __launch_bounds__(256) ell2_kernel(int nbr, const int* __restric
 // FSAI factors of a pressure system): one thread per row, slot-major coalesced
 // loads.  Float32 values times float32 x: each group of four slots is summed in
 // float32 and converted once, as the CSR kernel sums one 128-bit value load.
-template <int W, typename VT, typename XT, class Epi>
+template <int W, typename VT, typename XT, class Epi, int EB = 0>
 __global__ void __launch_bounds__(256) ell1_kernel(int n, const int* __restrict__ ec, const VT* __restrict__ ev,
-                                                   const XT* __restrict__ x, Epi epi) {
+                                                   const XT* __restrict__ x, Epi epi,
+                                                   const unsigned char* __restrict__ code = nullptr,
+                                                   const int* __restrict__ off = nullptr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int cc[W];
   VT vv[W];
 #pragma unroll
   for (int k = 0; k < W; ++k) {
-    cc[k] = __ldcs(ec + (long long)k * n + i);
+    cc[k] = slot_col<EB>(ec, code, off, (long long)k * n + i, i);
     vv[k] = __ldcs(ev + (long long)k * n + i);
   }
   double sum = 0.0;
@@ -446,8 +469,16 @@ void launch_ell1(cudaStream_t st, const deco_csr_s* A, const XT* x, Epi epi) {
   const VT* ev;
   if constexpr (sizeof(VT) == 4) ev = A->ev32.get(); else ev = A->ev.get();
   const unsigned grid = (unsigned)cdiv(A->n, 256);
-  if (A->ew == 4) ell1_kernel<4, VT, XT, Epi><<<grid, 256, 0, st>>>(A->n, A->ec.get(), ev, x, epi);
-  else ell1_kernel<8, VT, XT, Epi><<<grid, 256, 0, st>>>(A->n, A->ec.get(), ev, x, epi);
+  const unsigned char* cd = A->ecode.get();
+  const int* of = A->eoff.get();
+  auto go = [&](auto eb) {
+    constexpr int EB = decltype(eb)::value;
+    if (A->ew == 4) ell1_kernel<4, VT, XT, Epi, EB><<<grid, 256, 0, st>>>(A->n, A->ec.get(), ev, x, epi, cd, of);
+    else ell1_kernel<8, VT, XT, Epi, EB><<<grid, 256, 0, st>>>(A->n, A->ec.get(), ev, x, epi, cd, of);
+  };
+  if (A->eb == 1) go(std::integral_constant<int, 1>{});
+  else if (A->eb == 2) go(std::integral_constant<int, 2>{});
+  else go(std::integral_constant<int, 0>{});
   DECO_CHECK_LAUNCH();
 }
 
@@ -458,16 +489,24 @@ void launch_ell2(cudaStream_t st, const deco_csr_s* A, bool row0, const XT* x, E
   const VT* ev;
   if constexpr (sizeof(VT) == 4) ev = A->ev32.get(); else ev = A->ev.get();
   const unsigned grid = (unsigned)cdiv(nbr, 256);
-  if (A->ew == 4) {
-    if (row0) ell2_kernel<4, true, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi);
-    else ell2_kernel<4, false, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi);
-  } else if (A->ew == 7) {
-    if (row0) ell2_kernel<7, true, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi);
-    else ell2_kernel<7, false, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi);
-  } else {
-    if (row0) ell2_kernel<8, true, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi);
-    else ell2_kernel<8, false, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi);
-  }
+  const unsigned char* cd = A->ecode.get();
+  const int* of = A->eoff.get();
+  auto go = [&](auto eb) {
+    constexpr int EB = decltype(eb)::value;
+    if (A->ew == 4) {
+      if (row0) ell2_kernel<4, true, VT, XT, Epi, EB><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, cd, of);
+      else ell2_kernel<4, false, VT, XT, Epi, EB><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, cd, of);
+    } else if (A->ew == 7) {
+      if (row0) ell2_kernel<7, true, VT, XT, Epi, EB><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, cd, of);
+      else ell2_kernel<7, false, VT, XT, Epi, EB><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, cd, of);
+    } else {
+      if (row0) ell2_kernel<8, true, VT, XT, Epi, EB><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, cd, of);
+      else ell2_kernel<8, false, VT, XT, Epi, EB><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, cd, of);
+    }
+  };
+  if (A->eb == 1) go(std::integral_constant<int, 1>{});
+  else if (A->eb == 2) go(std::integral_constant<int, 2>{});
+  else go(std::integral_constant<int, 0>{});
   DECO_CHECK_LAUNCH();
 }
 
@@ -555,6 +594,11 @@ void make_padded(deco_ctx_s* ctx, deco_csr_s* A);
 // row has more than 4 entries, 8 when none has more than 8 and the padding stays
 // within 25 %), float32 values too when A has them; make_f32_values refreshes it.
 void make_padded_scalar(deco_ctx_s* ctx, deco_csr_s* A);
+// Offset codes of the slot columns of A's padded copy (nrow = cells for 2x2
+// blocks, rows for scalar rows): 1-byte codes when at most 256 distinct column
+// offsets occur, 2-byte codes up to 65536, none otherwise (and none when
+// ctx->slot_codes is off).  make_padded and make_padded_scalar call it.
+void make_slot_codes(deco_ctx_s* ctx, deco_csr_s* A, int nrow);
 void drop_bsr(deco_csr_s* A);
 
 // y = op(A x) over rows 0, bs, 2bs, ... (nrows_out = n / bs rows).  Uses the

@@ -119,6 +119,13 @@ int deco_csr_padded(deco_csr A, int* slots);
  * 5 % faster; DECO_AUTOTUNE=0 keeps the rules).  No counterpart in the
  * reference. */
 int deco_csr_product_plan(deco_csr A, int precision, int* kind, int* lanes);
+/* Bytes per slot column the padded products read: 1 or 2 when the slots'
+ * column offsets (column minus the slot's own row or cell) take at most 256 or
+ * 65536 distinct values and the copy stores a code per slot and the offsets
+ * once (`noffsets` of them), 4 when it stores the columns themselves, 0 without
+ * a padded copy.  DECO_SLOT_CODES=0 at context creation keeps 4-byte columns.
+ * No counterpart in the reference. */
+int deco_csr_slot_codes(deco_csr A, int* bytes, int* noffsets);
 
 /* y = A x (bs == 1), or the restricted product of alg::spmv with bs > 1:
  * y[i/bs] = (A x)[i] for rows i = 0, bs, 2bs, ...   (core/alg.hpp:50-64,
@@ -149,6 +156,9 @@ int deco_fsai_blocks(deco_fsai F, int* bs, int* nblk_lower, int* nblk_upper);
  * power-1 factors of 7-point systems, 0 without.  No counterpart in the
  * reference. */
 int deco_fsai_padded(deco_fsai F, int* slots_lower, int* slots_upper);
+/* Bytes per slot column of FL's and FU^T's padded copies (deco_csr_slot_codes).
+ * No counterpart in the reference. */
+int deco_fsai_slot_codes(deco_fsai F, int* bytes_lower, int* bytes_upper);
 /* FL (lower, diagonal last) and FU^T (upper) in the reference's layout. */
 int deco_fsai_download(deco_ctx ctx, deco_fsai F, int* h_Lr, int* h_Lc, double* h_Lv, int* h_Ur, int* h_Uc,
                        double* h_Uv);

@@ -164,3 +164,32 @@ def test_product_plan_chosen_by_the_cpr_autotuner(d, precision):
         x = P.apply(torch.from_numpy(rv).cuda()).cpu().numpy()
         xo = O.apply(rv)
         assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-12
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_slot_codes_give_bit_identical_solves(d, precision):
+    """On a 7-point stencil the slots' column offsets take a handful of values, so the
+    padded copies store 1-byte codes instead of 4-byte columns: the CPR setup and the
+    solve must match a context that keeps 4-byte columns (DECO_SLOT_CODES=0) bit for bit."""
+    import os
+    from conftest import cpr_json, sol_json
+    s = gen.generate(gen.preset(1))
+    out = []
+    for codes in ("1", "0"):
+        os.environ["DECO_SLOT_CODES"] = codes
+        try:
+            ctx = d.Context(0)
+        finally:
+            os.environ.pop("DECO_SLOT_CODES", None)
+        A = d.CSR.from_system(s, ctx)
+        b = torch.from_numpy(s.b.copy()).cuda()
+        P = d.CPR(cpr_json(2), A, b, precision=precision)
+        S = d.SOL(sol_json(), A, P, b, precision=precision)
+        ctx.sync()
+        out.append((A.slot_codes, S.iter, S.x.cpu().numpy()))
+    (bytes_on, noff_on), it_on, x_on = out[0]
+    (bytes_off, _), it_off, x_off = out[1]
+    assert bytes_on == 1 and 1 <= noff_on <= 256, out[0][0]
+    assert bytes_off == 4
+    assert it_on == it_off
+    np.testing.assert_array_equal(x_on, x_off)
