@@ -756,7 +756,7 @@ def main():
     for k in kernels.values():
         k["frac_of_peak"] = k["gbs"] / peak
     dom = kernels["spmv_A_f32"]
-    padded = dom["format"].endswith("slots per cell")
+    padded = "padded slots per cell" in dom["format"]
     kname = ("ell2_kernel<%d, float>" % int(dom["format"].split(", ")[1].split()[0])) if padded else None
     traffic, tsrc = dram_traffic(kname) if kname else (None, None)
     roofline = {"bound": "hbm", "achieved": dom["gbs"], "peak": peak, "unit": "GB/s", "frac": dom["gbs"] / peak,
