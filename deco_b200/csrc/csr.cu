@@ -95,7 +95,8 @@ __global__ void ell2_fill(int nbr, int W, const int* __restrict__ br, const int*
 // kMaxCodes distinct offsets appear the set stops growing and the count says so.
 constexpr int kSetCap = 1 << 17;
 constexpr int kMaxCodes = 1 << 16;
-constexpr int kSetEmpty = (int)0x80808080u;  // what a 0x80 byte fill leaves (no offset of an int32-indexed matrix reaches it)
+constexpr int kSetEmpty = (int)0x80808080u;
+constexpr long long kMinCodedSlots = 1LL << 22;  // what a 0x80 byte fill leaves (no offset of an int32-indexed matrix reaches it)
 
 __global__ void slot_offset_set(long long total, int nrow, const int* __restrict__ ec, int* __restrict__ set,
                                 int* __restrict__ count) {
@@ -152,6 +153,10 @@ void make_slot_codes(deco_ctx_s* ctx, deco_csr_s* A, int nrow) {
   if (!ctx->slot_codes || !A->ew || nrow <= 0 || !A->ec) return;
   cudaStream_t st = ctx->stream;
   const long long total = (long long)A->ew * nrow;
+  // below a few million slots a product is bound by its launch and tail, not by
+  // the column bytes, and building the codes (two passes and two host round
+  // trips) would cost more than it saves
+  if (total < kMinCodedSlots) return;
   DevBuf<int> set(kSetCap, st), count(1, st);
   DECO_CUDA(cudaMemsetAsync(set.get(), 0x80, sizeof(int) * kSetCap, st));  // every entry kSetEmpty
   count.zero(st);

@@ -123,7 +123,9 @@ int deco_csr_product_plan(deco_csr A, int precision, int* kind, int* lanes);
  * column offsets (column minus the slot's own row or cell) take at most 256 or
  * 65536 distinct values and the copy stores a code per slot and the offsets
  * once (`noffsets` of them), 4 when it stores the columns themselves, 0 without
- * a padded copy.  DECO_SLOT_CODES=0 at context creation keeps 4-byte columns.
+ * a padded copy.  Copies of fewer than 2^22 slots keep 4-byte columns (their
+ * products are bound by launch and tail, not bytes), and so does every copy
+ * after DECO_SLOT_CODES=0 at context creation.
  * No counterpart in the reference. */
 int deco_csr_slot_codes(deco_csr A, int* bytes, int* noffsets);
 

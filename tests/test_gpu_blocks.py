@@ -173,7 +173,7 @@ def test_slot_codes_give_bit_identical_solves(d, precision):
     solve must match a context that keeps 4-byte columns (DECO_SLOT_CODES=0) bit for bit."""
     import os
     from conftest import cpr_json, sol_json
-    s = gen.generate(gen.preset(1))
+    s = gen.grid(128, 100, 50, bs=2, seed=5)  # 640k cells: 7 slots x 640k, past the 2^22-slot coding threshold
     out = []
     for codes in ("1", "0"):
         os.environ["DECO_SLOT_CODES"] = codes
