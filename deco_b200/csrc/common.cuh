@@ -10,6 +10,7 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "deco_b200.h"
@@ -189,6 +190,53 @@ inline int grid_for(const deco_ctx_s* ctx, long long work, int block, int per_sm
   long long cap = (long long)ctx->num_sms * per_sm;
   if (g > cap) g = cap;
   return int(g < 1 ? 1 : g);
+}
+
+// ------------------------------------------- programmatic dependent launch
+// Inside a GMRES solve (and only there: the matrices are constant while it
+// runs) the kernels of an iteration are launched with programmatic stream
+// serialisation: a kernel's blocks may be scheduled while its predecessor's
+// last wave still runs.  Every kernel launched that way follows one protocol:
+//   * before pdl_wait() it reads only data written two or more kernels earlier
+//     (the matrices, older basis columns) and writes nothing;
+//   * pdl_wait() returns once the predecessor has completed and its writes are
+//     visible; pdl_trigger() comes after it, so when a kernel is launched the
+//     kernel two places before it has completed.
+// The slot-padded products load their matrix slots before the wait, so the
+// first blocks of a product stream the matrix during the tail of the kernel
+// before it.  A kernel launched without the attribute runs in plain stream
+// order and the two instructions are no-ops for it.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
+// true while the calling thread runs a solve with programmatic launches
+// (PdlScope; DECO_PDL=0 turns them off)
+bool pdl_active();
+struct PdlScope {
+  bool prev;
+  explicit PdlScope(bool on);
+  ~PdlScope();
+};
+
+// Launches kernel k (a kernel that follows the protocol above) with the
+// programmatic-serialisation attribute when pdl_active(), else as <<<...>>>.
+template <typename... KP, typename... Args>
+void launch_k(void (*k)(KP...), dim3 grid, dim3 block, size_t shm, cudaStream_t s, Args&&... args) {
+  if (pdl_active()) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = shm;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    DECO_CUDA(cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...));
+  } else {
+    k<<<grid, block, shm, s>>>(std::forward<Args>(args)...);
+  }
 }
 
 }  // namespace deco

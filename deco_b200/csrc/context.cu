@@ -16,6 +16,19 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 static std::atomic<long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
+// programmatic dependent launch inside solves (common.cuh)
+static thread_local bool t_pdl = false;
+static bool pdl_allowed() {
+  static const bool on = [] {
+    const char* e = std::getenv("DECO_PDL");
+    return !(e && std::atoi(e) == 0);
+  }();
+  return on;
+}
+bool pdl_active() { return t_pdl; }
+PdlScope::PdlScope(bool on) : prev(t_pdl) { t_pdl = on && pdl_allowed(); }
+PdlScope::~PdlScope() { t_pdl = prev; }
+
 // ------------------------------------------------------------ block cache
 namespace {
 std::mutex g_cache_mu;

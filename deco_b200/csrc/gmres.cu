@@ -24,6 +24,7 @@
 // rotations in float64; every restart recomputes the true residual b - A x and
 // the solution update in float64 (iterative refinement).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <mutex>
@@ -49,10 +50,14 @@ constexpr int kColsD = kWarps * 8;  // columns one block row of the dot pass tak
 // (j (j + 1) / 2 + j + 1 doubles, under the 227 KB opt-in limit); past it the
 // same arithmetic reads H from global memory
 constexpr int kBacksolveShm = 200;
-// host read-back of |g_{j+1}|: a ring of kRing pinned slots (from kSlot0) and
-// events; the host runs up to `lookahead` Arnoldi steps ahead (<= kRing - 2)
+// host read-back of |g_{j+1}|: a ring of kRing pinned slots (values from kSlot0,
+// tags from kTag0) that the update pass writes; the host runs up to `lookahead`
+// Arnoldi steps ahead (<= kRing - 2)
 constexpr int kRing = 8;
 constexpr int kSlot0 = 4;
+constexpr int kTag0 = 24;  // the ring's tags (8-byte words of the context's pinned buffer)
+// step tags, unique in the process, so a slot never matches an earlier solve's post
+std::atomic<unsigned long long> g_step_tag{0};
 constexpr double kEps = 2.220446049250312e-16;
 
 // device state (float64): H (m+1)*m | G (m+1)^2 | g | cs | sn | s | c | sums 2(m+2) | sc
@@ -78,6 +83,22 @@ struct State {
   }
 };
 enum { SC_RES = 0, SC_BREAK = 1, SC_BETA = 2 };
+
+// |g_{j+1}| of Arnoldi step j posted straight into pinned host memory by the
+// update pass (no copy or event in the stream between the step's last kernel
+// and the next step's first, so those launch back to back): the value, a
+// system-scope fence, then a tag unique to the step.  The host polls the tag.
+struct HostSlot {
+  double* val = nullptr;              // device view of the pinned ring of values
+  unsigned long long* tag = nullptr;  // device view of the pinned ring of tags
+  unsigned long long t = 0;           // this step's tag
+  __device__ void post(double v) const {
+    if (!val) return;
+    *val = v;
+    __threadfence_system();
+    *reinterpret_cast<volatile unsigned long long*>(tag) = t;
+  }
+};
 
 
 // deterministic last-block reduction of red[i*nb + b] over b for i < ncols.
@@ -266,6 +287,10 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long 
 #pragma unroll
     for (int i = 0; i < kStages - 1; ++i) issue();
   }
+  // the copies above read basis columns only (written two or more kernels
+  // back); w is the predecessor's output
+  pdl_wait();
+  pdl_trigger();
   int cst = 0;  // the consumer's stage
   for (int ch = 0; ch < nch && nk > 0; ++ch) {
     const long long c0 = v0 + (long long)ch * kChunk + lane;
@@ -319,6 +344,186 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots(long long n, long long 
   dots_finish(ncols, j, red, st, hs);
 }
 
+// ---- pass A, float32 basis, through the bulk-copy (TMA) engine.
+// The same units, stages and sums as arnoldi_dots, but each unit (one chunk of
+// one column, up to 2 KB) is ONE cp.async.bulk issued by lane 0 of the warp,
+// completing on an mbarrier of its stage (transaction bytes); the lanes wait on
+// that barrier and read back the whole chunk.  The per-lane copy instructions
+// and their address arithmetic go away, which is what bounded the per-lane form
+// (an issue-rate limit at 16 warps per SM).  Each lane sums its vectors in the
+// same order as arnoldi_dots, so the dots are bit-identical.  Every wait on a
+// barrier is bounded: past kSpinLimit polls the kernel records SC_TIMEOUT,
+// stops issuing copies, and before returning waits (bounded again) for the
+// copies it has in flight.
+constexpr size_t kDotsBarBytes = (size_t)kWarps * kStages * sizeof(unsigned long long);
+constexpr unsigned kSpinLimit = 1u << 24;
+enum { SC_TIMEOUT = 3 };
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// true once the barrier's phase `parity` has completed, false after kSpinLimit polls
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* b, unsigned parity) {
+  for (unsigned it = 0; it < kSpinLimit; ++it)
+    if (mbar_try_wait(b, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ unsigned long long policy_evict_first() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+// global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* b,
+                                         unsigned long long policy) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;\n" ::
+          "r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(b)), "l"(policy)
+      : "memory");
+}
+
+template <int CPW>
+__global__ void __launch_bounds__(kThreads) arnoldi_dots_bulk(long long n, long long ld, int ncols, int j,
+                                                              const float* __restrict__ V, const float* __restrict__ w,
+                                                              double* __restrict__ red, unsigned* counter, State st) {
+  extern __shared__ __align__(128) unsigned char dots_smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float4* stg = reinterpret_cast<float4*>(dots_smem) + (size_t)warp * kStages * kChunk;
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(dots_smem + kDotsStageBytes) + warp * kStages;
+  double* hs = reinterpret_cast<double*>(dots_smem + kDotsStageBytes + kDotsBarBytes);  // ncols doubles
+  const int cbase = blockIdx.y * (kWarps * CPW);
+  int nk = 0;  // columns of this warp (uniform over its lanes)
+#pragma unroll
+  for (int k = 0; k < CPW; ++k) nk += (cbase + warp + k * kWarps < ncols) ? 1 : 0;
+  const long long nvec = n / 4;
+  const long long per = (nvec + gridDim.x - 1) / gridDim.x;
+  const long long v0 = min(nvec, per * blockIdx.x), v1 = min(nvec, v0 + per);
+  const int nvb = (int)(v1 - v0);  // 16-byte vectors of this block's row range
+  const int nch = (nvb + kChunk - 1) / kChunk;
+  const int nunits = nch * nk;
+  if (lane == 0) {
+#pragma unroll
+    for (int s = 0; s < kStages; ++s) mbar_init(bar + s, 1);
+    fence_async_shared();
+  }
+  __syncwarp();
+  const unsigned long long pol = policy_evict_first();
+  const float4* __restrict__ Vv = reinterpret_cast<const float4*>(V);
+  const long long ldv = ld / 4;
+  // producer cursor (kept by every lane, used by lane 0): next unit, its chunk,
+  // its column slot and its stage
+  int pu = 0, pch = 0, pk = 0, pst = 0;
+  bool dead = false;  // a barrier wait ran out: no further copies
+  auto issue = [&]() {
+    if (pu < nunits && !dead) {
+      if (lane == 0) {
+        const int off = pch * kChunk;
+        const unsigned bytes = (unsigned)min(kChunk, nvb - off) * 16u;
+        const float4* src = Vv + (size_t)(cbase + warp + pk * kWarps) * ldv + v0 + off;
+        fence_async_shared();  // the lanes' reads of this stage (ordered by __syncwarp) before the copy's writes
+        mbar_expect_tx(bar + pst, bytes);
+        bulk_g2s(stg + pst * kChunk, src, bytes, bar + pst, pol);
+      }
+      ++pu;
+      if (++pk == nk) { pk = 0; ++pch; }
+      if (++pst == kStages) pst = 0;
+    }
+  };
+#pragma unroll
+  for (int i = 0; i < kStages - 1; ++i) issue();
+  // the copies above read basis columns only (written two or more kernels
+  // back); w is the predecessor's output
+  pdl_wait();
+  pdl_trigger();
+  const float4* __restrict__ wv4 = reinterpret_cast<const float4*>(w);
+  const float4* __restrict__ uv4 = Vv + (size_t)j * ldv;
+  double pw[CPW], pq[CPW];
+#pragma unroll
+  for (int k = 0; k < CPW; ++k) { pw[k] = 0.0; pq[k] = 0.0; }
+  int cu = 0, cst = 0;  // the consumer's unit and stage
+  unsigned cph = 0;     // parity of the stage's current phase (flips when cst wraps)
+  for (int ch = 0; ch < nch && nk > 0 && !dead; ++ch) {
+    const int cnt = min(kChunk, nvb - ch * kChunk);
+    const long long c0 = v0 + (long long)ch * kChunk + lane;
+    float4 wv[kVecPerLane], uv[kVecPerLane];
+#pragma unroll
+    for (int q = 0; q < kVecPerLane; ++q) {
+      const bool in = lane + q * 32 < cnt;
+      wv[q] = in ? __ldg(wv4 + c0 + q * 32) : make_float4(0.f, 0.f, 0.f, 0.f);
+      uv[q] = in ? __ldg(uv4 + c0 + q * 32) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int k = 0; k < CPW; ++k) {
+      if (k < nk && !dead) {
+        issue();  // unit cu + kStages - 1 into the stage unit cu - 1 used
+        // the verdict is made warp-uniform, so the lanes stay converged
+        if (!__all_sync(0xffffffffu, mbar_wait_bounded(bar + cst, cph))) {
+          dead = true;
+          if (lane == 0) st.sc[SC_TIMEOUT] = 1.0;
+          break;
+        }
+        const float4* src = stg + cst * kChunk;
+#pragma unroll
+        for (int q = 0; q < kVecPerLane; ++q) {
+          if (lane + q * 32 < cnt) {
+            const float4 v = src[q * 32 + lane];
+            pw[k] += vdot(v, wv[q]);
+            pq[k] += vdot(v, uv[q]);
+          }
+        }
+        __syncwarp();
+        ++cu;
+        if (++cst == kStages) { cst = 0; cph ^= 1u; }
+      }
+    }
+  }
+  if (dead) {  // let the copies in flight land before the block's shared memory goes away
+    for (; cu < pu; ++cu) {
+      mbar_wait_bounded(bar + cst, cph);
+      if (++cst == kStages) { cst = 0; cph ^= 1u; }
+    }
+  }
+  if (blockIdx.x == gridDim.x - 1 && lane == 0) {  // rows past the last full vector
+    const float* __restrict__ uj = V + (size_t)j * ld;
+    for (long long r = nvec * 4; r < n; ++r)
+#pragma unroll
+      for (int k = 0; k < CPW; ++k) {
+        const int c = cbase + warp + k * kWarps;
+        if (c < ncols) {
+          const double v = (double)V[(size_t)c * ld + r];
+          pw[k] += v * (double)w[r];
+          pq[k] += v * (double)uj[r];
+        }
+      }
+  }
+#pragma unroll
+  for (int k = 0; k < CPW; ++k) {
+    const int c = cbase + warp + k * kWarps;
+    const double a = warp_sum(pw[k]), b = warp_sum(pq[k]);
+    if (lane == 0 && c < ncols) {
+      red[(size_t)c * gridDim.x + blockIdx.x] = a;
+      red[(size_t)(ncols + c) * gridDim.x + blockIdx.x] = b;
+    }
+  }
+  if (!last_block(counter)) return;
+  dots_finish(ncols, j, red, st, hs);
+}
+
 // ---- pass A for the float64 basis: the same dots with w and u_j held in
 // registers: warp w owns columns w, w+8, ...; each lane loads its 128-bit vectors
 // of w and u_j once per step and streams its columns against them (no barriers;
@@ -331,6 +536,8 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots_reg(long long n, long l
                                                              double* __restrict__ red, unsigned* counter, State st) {
   using VT = typename Vec4<T>::t;
   constexpr int N = Vec4<T>::N;
+  pdl_wait();
+  pdl_trigger();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int cbase = blockIdx.y * kColsD;  // block row y of the grid takes columns 64y .. 64y + 63
   const long long nvec = n / N;
@@ -395,8 +602,39 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots_reg(long long n, long l
   dots_finish(ncols, j, red, st, dyn_hs);
 }
 
-// the staged float32 dot pass needs more than the 48 KB of shared memory a block
-// gets by default: raise the limit once per (instantiation, device)
+// Dynamic shared memory that lets at most `blocks` blocks of a kernel share an
+// SM (and still lets `blocks` fit): the single-wave grid-stride passes size
+// their grids as `blocks` per SM, and under programmatic launch their blocks
+// are placed while the previous kernel still holds part of the GPU; if an SM
+// could take more, the early SMs fill up and the grid's equal shares pile on
+// fewer SMs.  (Measured on the 1.5M-row system: the float32 dot pass with room
+// for three blocks per SM took 0.330 ms per iteration against 0.259 ms capped.)
+size_t smem_for_blocks(int blocks, size_t need, size_t static_bytes) {
+  static std::mutex mu;
+  static std::vector<std::pair<int, int>> per_dev;  // (shared memory per SM, reserved per block)
+  int dev = 0;
+  DECO_CUDA(cudaGetDevice(&dev));
+  std::pair<int, int> a;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)per_dev.size() <= dev) per_dev.resize(dev + 1, {0, 0});
+    if (!per_dev[dev].first) {
+      DECO_CUDA(cudaDeviceGetAttribute(&per_dev[dev].first, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+      DECO_CUDA(cudaDeviceGetAttribute(&per_dev[dev].second, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+    }
+    a = per_dev[dev];
+  }
+  const size_t sm = (size_t)a.first, res = (size_t)a.second + static_bytes;
+  size_t cap = sm / (blocks + 1) + 16 - res;  // blocks + 1 no longer fit
+  cap = (cap + 15) / 16 * 16;
+  if (need >= cap || (size_t)blocks * (cap + res) > sm) return need;
+  return cap;
+}
+
+constexpr size_t kDotsShmMax = 96 * 1024;  // the dot passes' dynamic shared memory limit
+
+// the staged float32 dot passes need more than the 48 KB of shared memory a
+// block gets by default: raise the limit once per (instantiation, device)
 template <int CPW>
 void allow_dots_smem() {
   static std::mutex mu;
@@ -406,9 +644,29 @@ void allow_dots_smem() {
   std::lock_guard<std::mutex> lk(mu);
   if ((int)done.size() <= dev) done.resize(dev + 1, 0);
   if (done[dev]) return;
+  static_assert(kDotsStageBytes + kDotsBarBytes + sizeof(double) * (kMaxRestart + 1) <= kDotsShmMax, "dot pass smem");
   DECO_CUDA(cudaFuncSetAttribute(arnoldi_dots<float, CPW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(kDotsStageBytes + sizeof(double) * (kMaxRestart + 1))));
+                                 (int)kDotsShmMax));
+  DECO_CUDA(cudaFuncSetAttribute(arnoldi_dots_bulk<CPW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kDotsShmMax));
   done[dev] = 1;
+}
+
+// The float32 dot pass at two blocks per SM: the per-lane cp.async form for up
+// to 16 columns, the bulk-copy form from 17 (measured per launch on the 4M-row
+// system: 33.5 / 50.8 us per-lane against 36.4 / 52.2 us bulk at 1 and 2
+// columns per warp, 86.9 against 77.8 us at 4).
+template <int CPW>
+void launch_dots_f32(cudaStream_t s, dim3 grid, size_t shm, long long n, long long ld, int nc, int j, const float* V,
+                     const float* w, double* red, unsigned* counter, State st) {
+  allow_dots_smem<CPW>();
+  constexpr size_t kStatic = 64;  // the kernels' static shared memory (last-block flag), rounded up
+  if (CPW >= 4)
+    launch_k(arnoldi_dots_bulk<CPW>, grid, kThreads, smem_for_blocks(2, kDotsStageBytes + kDotsBarBytes + shm, kStatic),
+             s, n, ld, nc, j, V, w, red, counter, st);
+  else
+    launch_k(arnoldi_dots<float, CPW>, grid, kThreads, smem_for_blocks(2, kDotsStageBytes + shm, kStatic), s, n, ld, nc,
+             j, V, w, red, counter, st);
 }
 
 template <typename T>
@@ -416,27 +674,17 @@ void launch_arnoldi_dots(cudaStream_t s, int nb, long long n, long long ld, int 
                          double* red, unsigned* counter, State st) {
   const size_t shm = sizeof(double) * (size_t)nc;  // h for the last block (dots_finish)
   if constexpr (std::is_same<T, double>::value) {
-    arnoldi_dots_reg<T><<<dim3(nb, (nc + kColsD - 1) / kColsD), kThreads, shm, s>>>(n, ld, nc, j, V, w, red, counter,
-                                                                                   st);
+    launch_k(arnoldi_dots_reg<T>, dim3(nb, (nc + kColsD - 1) / kColsD), kThreads, shm, s, n, ld, nc, j, V, w, red,
+             counter, st);
   } else {
     // two blocks per SM of 64 KB stages each (measured at restart 50 on 8M rows:
     // 0.160 ms per step against 0.170 with three blocks per SM)
     const int nbd = nb / 2;
-    const size_t shs = kDotsStageBytes + shm;
-    if (nc <= kWarps) {
-      allow_dots_smem<1>();
-      arnoldi_dots<T, 1><<<nbd, kThreads, shs, s>>>(n, ld, nc, j, V, w, red, counter, st);
-    } else if (nc <= 2 * kWarps) {
-      allow_dots_smem<2>();
-      arnoldi_dots<T, 2><<<nbd, kThreads, shs, s>>>(n, ld, nc, j, V, w, red, counter, st);
-    } else if (nc <= 4 * kWarps) {
-      allow_dots_smem<4>();
-      arnoldi_dots<T, 4><<<nbd, kThreads, shs, s>>>(n, ld, nc, j, V, w, red, counter, st);
-    } else {  // 8 columns per warp; past 64 columns further block rows, 64 columns each
-      allow_dots_smem<8>();
-      arnoldi_dots<T, 8><<<dim3(nbd, (nc + kColsD - 1) / kColsD), kThreads, shs, s>>>(n, ld, nc, j, V, w, red,
-                                                                                      counter, st);
-    }
+    if (nc <= kWarps) launch_dots_f32<1>(s, nbd, shm, n, ld, nc, j, V, w, red, counter, st);
+    else if (nc <= 2 * kWarps) launch_dots_f32<2>(s, nbd, shm, n, ld, nc, j, V, w, red, counter, st);
+    else if (nc <= 4 * kWarps) launch_dots_f32<4>(s, nbd, shm, n, ld, nc, j, V, w, red, counter, st);
+    else  // 8 columns per warp; past 64 columns further block rows, 64 columns each
+      launch_dots_f32<8>(s, dim3(nbd, (nc + kColsD - 1) / kColsD), shm, n, ld, nc, j, V, w, red, counter, st);
   }
 }
 
@@ -452,11 +700,13 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) arnoldi_update(long long n, long long ld, int ncols, int j,
                                                            const T* __restrict__ V, const T* __restrict__ w,
                                                            T* __restrict__ out, double* __restrict__ red,
-                                                           unsigned* counter, State st) {
+                                                           unsigned* counter, State st, HostSlot hs) {
   using VT = typename Vec4<T>::t;
   constexpr int N = Vec4<T>::N;
   constexpr int U = N == 4 ? 16 : 8;
   extern __shared__ double dyn_u[];
+  pdl_wait();
+  pdl_trigger();
   double* cs_ = dyn_u;
   for (int i = threadIdx.x; i < ncols; i += kThreads) cs_[i] = st.c[i];
   __syncthreads();
@@ -526,6 +776,7 @@ __global__ void __launch_bounds__(kThreads) arnoldi_update(long long n, long lon
     givens_apply(st.cs[j], st.sn[j], hc[j], hc[j + 1]);
     givens_apply(st.cs[j], st.sn[j], st.g[j], st.g[j + 1]);
     st.sc[SC_RES] = fabs(st.g[j + 1]);
+    hs.post(st.sc[SC_RES]);
   }
   __syncthreads();
   for (int i = threadIdx.x; i <= j + 1; i += kThreads) st.h(i, j) = hc[i];
@@ -695,6 +946,12 @@ struct Solver {
   int lookahead = 3;  // Arnoldi steps queued beyond the one whose |g| the host is waiting for
   std::vector<cudaEvent_t> pev;
   double t_phase[3] = {0, 0, 0};
+  // the |g| ring: host views, device views, and the tag each slot waits for
+  volatile double* hval = nullptr;
+  volatile unsigned long long* htag = nullptr;
+  double* dval = nullptr;
+  unsigned long long* dtag = nullptr;
+  unsigned long long tags[kRing] = {};
   ~Solver() {
     for (auto e : pev) cudaEventDestroy(e);
   }
@@ -777,8 +1034,8 @@ struct Solver {
   }
 
   // Arnoldi step j: writes column j of H/G, g_{j+1}, rotation j and basis column
-  // j+1; |g_{j+1}| is copied to host slot j % kRing and ev[j % kRing] recorded after it.
-  void arnoldi_step(int j, bool left, volatile double* hsc, cudaEvent_t* ev) {
+  // j+1; the update pass posts |g_{j+1}| into host slot j % kRing with tag tags[j % kRing].
+  void arnoldi_step(int j, bool left) {
     cudaStream_t s = ctx->stream;
     const double* sj = st.s + j;
     // phase order per step: [pev0] precond [pev1] matvec [pev2] ortho [pev3]
@@ -797,17 +1054,41 @@ struct Solver {
     const int nc = j + 1;
     launch_arnoldi_dots<T>(s, nb, n, ld, nc, j, V.get(), w.get(), ctx->red.get(), ctx->counter.get(), st);
     DECO_CHECK_LAUNCH();
-    arnoldi_update<T><<<nb, kThreads, sizeof(double) * 4 * (nc + 1), s>>>(n, ld, nc, j, V.get(), w.get(), col(j + 1),
-                                                                           ctx->red.get(), ctx->counter.get(), st);
+    HostSlot hs;
+    hs.val = dval + j % kRing;
+    hs.tag = dtag + j % kRing;
+    hs.t = tags[j % kRing] = g_step_tag.fetch_add(1, std::memory_order_relaxed) + 1;
+    // nb = 4 blocks per SM (smem_for_blocks: no fifth block on an SM)
+    launch_k(arnoldi_update<T>, nb, kThreads, smem_for_blocks(4, sizeof(double) * 4 * (nc + 1), 128), s, n, ld, nc, j,
+             V.get(), w.get(), col(j + 1), ctx->red.get(), ctx->counter.get(), st, hs);
     DECO_CHECK_LAUNCH();
     if (profile) DECO_CUDA(cudaEventRecord(pev[4 * j + 3], s));
-    DECO_CUDA(cudaMemcpyAsync(const_cast<double*>(hsc) + kSlot0 + j % kRing, st.sc + SC_RES, sizeof(double),
-                              cudaMemcpyDeviceToHost, s));
-    DECO_CUDA(cudaEventRecord(ev[j % kRing], s));
+  }
+
+  // |g_{j+1}| of step j, once the update pass has posted it.  The host polls
+  // the tag; every 1024 polls it asks the stream whether it failed or drained.
+  double step_result(int j) {
+    const int slot = j % kRing;
+    volatile unsigned long long* tp = htag + slot;
+    for (unsigned long long spin = 1; *tp != tags[slot]; ++spin) {
+      if ((spin & 1023) == 0) {
+        const cudaError_t e = cudaStreamQuery(ctx->stream);
+        if (e == cudaSuccess) {
+          if (*tp == tags[slot]) break;
+          throw Error(DECO_ERR_INTERNAL, "gmres: an Arnoldi step finished without posting its residual");
+        }
+        if (e != cudaErrorNotReady) DECO_CUDA(e);
+      }
+    }
+    std::atomic_thread_fence(std::memory_order_acquire);
+    return hval[slot];
   }
 
   void run(const double* b, double* x, deco_sol_result* res, double* resvec) {
     cudaStream_t s = ctx->stream;
+    // the iteration's products and Arnoldi passes launch programmatically
+    // (common.cuh): A and the preconditioner stay constant from here on
+    PdlScope pdl(true);
     const bool left = prm.type == 1;
     const int itmax = prm.itmax;
     double* r = r64.get();
@@ -825,14 +1106,15 @@ struct Solver {
     int flag = 1, iter = 0, restarts = 0;
     double rnorm = 0.0;
     volatile double* hsc = ctx->host_scalars;
-    cudaEvent_t ev[kRing];
-    for (auto& e : ev) DECO_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    struct EvGuard {
-      cudaEvent_t* e;
-      ~EvGuard() {
-        for (int i = 0; i < kRing; ++i) cudaEventDestroy(e[i]);
-      }
-    } evg{ev};
+    // the ring of posted |g| values and their tags in the context's pinned buffer
+    hval = hsc + kSlot0;
+    htag = reinterpret_cast<volatile unsigned long long*>(ctx->host_scalars + kTag0);
+    {
+      void* d = nullptr;
+      DECO_CUDA(cudaHostGetDevicePointer(&d, ctx->host_scalars, 0));
+      dval = static_cast<double*>(d) + kSlot0;
+      dtag = reinterpret_cast<unsigned long long*>(static_cast<double*>(d) + kTag0);
+    }
     while (iter < itmax) {
       DECO_CUDA(cudaMemsetAsync(st_buf.get(), 0, sizeof(double) * State::doubles(m), s));
       start_cycle<T><<<nb, kThreads, 0, s>>>(n, r, col(0), ctx->red.get(), ctx->counter.get(), st, norm.get());
@@ -850,15 +1132,12 @@ struct Solver {
       for (;;) {
         if (!(j < m && base + j < itmax)) break;
         double gj = hsc[2];  // |g_0|; step 0 is launched only after it is checked
-        if (j > 0) {
-          DECO_CUDA(cudaEventSynchronize(ev[(j - 1) % kRing]));
-          gj = hsc[kSlot0 + (j - 1) % kRing];
-        }
+        if (j > 0) gj = step_result(j - 1);
         rnorm = fabs(gj);
         if (resvec) resvec[base + j] = rnorm / bnorm;
         if (rnorm < abstol) { flag = 0; break; }
         while (launched < m && base + launched < itmax && launched <= j + lookahead) {
-          arnoldi_step(launched, left, hsc, ev);
+          arnoldi_step(launched, left);
           ++launched;
         }
         ++j;
@@ -866,9 +1145,13 @@ struct Solver {
       iter = base + j;
       launch_backsolve(s, st, j);
       DECO_CHECK_LAUNCH();
-      DECO_CUDA(cudaMemcpyAsync(const_cast<double*>(hsc) + 3, st.sc + SC_BREAK, sizeof(double), cudaMemcpyDeviceToHost, s));
+      // sc[SC_BREAK .. SC_TIMEOUT] -> hsc[16 ..]
+      DECO_CUDA(cudaMemcpyAsync(const_cast<double*>(hsc) + 16, st.sc + SC_BREAK,
+                                sizeof(double) * (SC_TIMEOUT - SC_BREAK + 1), cudaMemcpyDeviceToHost, s));
       DECO_CUDA(cudaStreamSynchronize(s));
-      if (hsc[3] != 0.0)
+      if (hsc[16 + SC_TIMEOUT - SC_BREAK] != 0.0)
+        throw Error(DECO_ERR_CUDA, "Arnoldi dot pass: a bulk copy into shared memory did not complete");
+      if (hsc[16] != 0.0)
         throw Error(DECO_ERR_BREAKDOWN, "Error in rgmres: Zero diagonal element in upper triangular matrix.");
       collect(launched);
       combine<T, double><<<nb, kThreads, sizeof(double) * (j > 0 ? j : 1), s>>>(n, ld, j > 0 ? j : 1, V.get(), st.c,

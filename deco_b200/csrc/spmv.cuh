@@ -136,6 +136,8 @@ __global__ void __launch_bounds__(256) spmv_kernel(int nrows_out, int row_stride
   using VV = typename Vec<VT>::V;
   using VI = typename Vec<VT>::I;
   constexpr int W = Vec<VT>::W;
+  pdl_wait();
+  pdl_trigger();
   const int lane = threadIdx.x & (SW - 1);
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int orow = int(gid / SW);
@@ -177,12 +179,12 @@ void launch_spmv_sw(cudaStream_t st, int sw, int nrows_out, int row_stride, cons
   const long long threads = (long long)nrows_out * sw;
   const unsigned grid = (unsigned)cdiv(threads, block);
   switch (sw) {
-    case 1: spmv_kernel<1, VT, XT, Epi><<<grid, block, 0, st>>>(nrows_out, row_stride, r, c, v, x, epi); break;
-    case 2: spmv_kernel<2, VT, XT, Epi><<<grid, block, 0, st>>>(nrows_out, row_stride, r, c, v, x, epi); break;
-    case 4: spmv_kernel<4, VT, XT, Epi><<<grid, block, 0, st>>>(nrows_out, row_stride, r, c, v, x, epi); break;
-    case 8: spmv_kernel<8, VT, XT, Epi><<<grid, block, 0, st>>>(nrows_out, row_stride, r, c, v, x, epi); break;
-    case 16: spmv_kernel<16, VT, XT, Epi><<<grid, block, 0, st>>>(nrows_out, row_stride, r, c, v, x, epi); break;
-    default: spmv_kernel<32, VT, XT, Epi><<<grid, block, 0, st>>>(nrows_out, row_stride, r, c, v, x, epi); break;
+    case 1: launch_k(spmv_kernel<1, VT, XT, Epi>, grid, block, 0, st, nrows_out, row_stride, r, c, v, x, epi); break;
+    case 2: launch_k(spmv_kernel<2, VT, XT, Epi>, grid, block, 0, st, nrows_out, row_stride, r, c, v, x, epi); break;
+    case 4: launch_k(spmv_kernel<4, VT, XT, Epi>, grid, block, 0, st, nrows_out, row_stride, r, c, v, x, epi); break;
+    case 8: launch_k(spmv_kernel<8, VT, XT, Epi>, grid, block, 0, st, nrows_out, row_stride, r, c, v, x, epi); break;
+    case 16: launch_k(spmv_kernel<16, VT, XT, Epi>, grid, block, 0, st, nrows_out, row_stride, r, c, v, x, epi); break;
+    default: launch_k(spmv_kernel<32, VT, XT, Epi>, grid, block, 0, st, nrows_out, row_stride, r, c, v, x, epi); break;
   }
   DECO_CHECK_LAUNCH();
 }
@@ -202,6 +204,8 @@ __global__ void __launch_bounds__(256) bsr_kernel(int nbr, const int* __restrict
                                                   const VT* __restrict__ bv, long long plane,
                                                   const XT* __restrict__ x, Epi epi) {
   constexpr int NR = ROW0 ? 1 : BS;
+  pdl_wait();
+  pdl_trigger();
   const int lane = threadIdx.x & (SW - 1);
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int s = int(gid / SW);
@@ -337,6 +341,8 @@ template <int SW, bool ROW0, typename VT, typename XT, class Epi>
 __global__ void __launch_bounds__(256) bsr2_pair_kernel(int nbr, const int* __restrict__ br, const int* __restrict__ bc,
                                                         const VT* __restrict__ bv, long long plane,
                                                         const XT* __restrict__ x, Epi epi) {
+  pdl_wait();
+  pdl_trigger();
   const int lane = threadIdx.x & (SW - 1);
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int s = int(gid / SW);
@@ -405,6 +411,10 @@ __global__ void __launch_bounds__(256) ell2_kernel(int nbr, const int* __restric
     a[k] = __ldcs(e2 + (long long)k * nbr + s);
     if (!ROW0) b[k] = __ldcs(e2 + (long long)(W + k) * nbr + s);
   }
+  // the matrix slots above are constant during a solve; x and the epilogue's
+  // vectors may be the predecessor's output
+  pdl_wait();
+  pdl_trigger();
   double s0 = 0.0, s1 = 0.0;
 #pragma unroll
   for (int k = 0; k < W; ++k) {
@@ -447,6 +457,8 @@ __global__ void __launch_bounds__(256) ell1_kernel(int n, const int* __restrict_
     cc[k] = slot_col<EB>(ec, code, off, (long long)k * n + i, i);
     vv[k] = __ldcs(ev + (long long)k * n + i);
   }
+  pdl_wait();
+  pdl_trigger();
   double sum = 0.0;
   if constexpr (kRunF32<VT, XT>) {
 #pragma unroll
@@ -473,8 +485,8 @@ void launch_ell1(cudaStream_t st, const deco_csr_s* A, const XT* x, Epi epi) {
   const int* of = A->eoff.get();
   auto go = [&](auto eb) {
     constexpr int EB = decltype(eb)::value;
-    if (A->ew == 4) ell1_kernel<4, VT, XT, Epi, EB><<<grid, 256, 0, st>>>(A->n, A->ec.get(), ev, x, epi, cd, of);
-    else ell1_kernel<8, VT, XT, Epi, EB><<<grid, 256, 0, st>>>(A->n, A->ec.get(), ev, x, epi, cd, of);
+    if (A->ew == 4) launch_k(ell1_kernel<4, VT, XT, Epi, EB>, grid, 256, 0, st, A->n, A->ec.get(), ev, x, epi, cd, of);
+    else launch_k(ell1_kernel<8, VT, XT, Epi, EB>, grid, 256, 0, st, A->n, A->ec.get(), ev, x, epi, cd, of);
   };
   if (A->eb == 1) go(std::integral_constant<int, 1>{});
   else if (A->eb == 2) go(std::integral_constant<int, 2>{});
@@ -494,14 +506,14 @@ void launch_ell2(cudaStream_t st, const deco_csr_s* A, bool row0, const XT* x, E
   auto go = [&](auto eb) {
     constexpr int EB = decltype(eb)::value;
     if (A->ew == 4) {
-      if (row0) ell2_kernel<4, true, VT, XT, Epi, EB><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, cd, of);
-      else ell2_kernel<4, false, VT, XT, Epi, EB><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, cd, of);
+      if (row0) launch_k(ell2_kernel<4, true, VT, XT, Epi, EB>, grid, 256, 0, st, nbr, A->ec.get(), ev, x, epi, cd, of);
+      else launch_k(ell2_kernel<4, false, VT, XT, Epi, EB>, grid, 256, 0, st, nbr, A->ec.get(), ev, x, epi, cd, of);
     } else if (A->ew == 7) {
-      if (row0) ell2_kernel<7, true, VT, XT, Epi, EB><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, cd, of);
-      else ell2_kernel<7, false, VT, XT, Epi, EB><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, cd, of);
+      if (row0) launch_k(ell2_kernel<7, true, VT, XT, Epi, EB>, grid, 256, 0, st, nbr, A->ec.get(), ev, x, epi, cd, of);
+      else launch_k(ell2_kernel<7, false, VT, XT, Epi, EB>, grid, 256, 0, st, nbr, A->ec.get(), ev, x, epi, cd, of);
     } else {
-      if (row0) ell2_kernel<8, true, VT, XT, Epi, EB><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, cd, of);
-      else ell2_kernel<8, false, VT, XT, Epi, EB><<<grid, 256, 0, st>>>(nbr, A->ec.get(), ev, x, epi, cd, of);
+      if (row0) launch_k(ell2_kernel<8, true, VT, XT, Epi, EB>, grid, 256, 0, st, nbr, A->ec.get(), ev, x, epi, cd, of);
+      else launch_k(ell2_kernel<8, false, VT, XT, Epi, EB>, grid, 256, 0, st, nbr, A->ec.get(), ev, x, epi, cd, of);
     }
   };
   if (A->eb == 1) go(std::integral_constant<int, 1>{});
@@ -516,10 +528,10 @@ void launch_bsr_bs(cudaStream_t st, int sw, int nbr, const int* br, const int* b
   if constexpr (BS == 2) {
     const unsigned grid = (unsigned)cdiv((long long)nbr * sw, 256);
     switch (sw) {
-      case 1: bsr2_pair_kernel<1, ROW0, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, br, bc, bv, plane, x, epi); break;
-      case 2: bsr2_pair_kernel<2, ROW0, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, br, bc, bv, plane, x, epi); break;
-      case 4: bsr2_pair_kernel<4, ROW0, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, br, bc, bv, plane, x, epi); break;
-      default: bsr2_pair_kernel<8, ROW0, VT, XT, Epi><<<grid, 256, 0, st>>>(nbr, br, bc, bv, plane, x, epi); break;
+      case 1: launch_k(bsr2_pair_kernel<1, ROW0, VT, XT, Epi>, grid, 256, 0, st, nbr, br, bc, bv, plane, x, epi); break;
+      case 2: launch_k(bsr2_pair_kernel<2, ROW0, VT, XT, Epi>, grid, 256, 0, st, nbr, br, bc, bv, plane, x, epi); break;
+      case 4: launch_k(bsr2_pair_kernel<4, ROW0, VT, XT, Epi>, grid, 256, 0, st, nbr, br, bc, bv, plane, x, epi); break;
+      default: launch_k(bsr2_pair_kernel<8, ROW0, VT, XT, Epi>, grid, 256, 0, st, nbr, br, bc, bv, plane, x, epi); break;
     }
     DECO_CHECK_LAUNCH();
     return;
@@ -527,11 +539,11 @@ void launch_bsr_bs(cudaStream_t st, int sw, int nbr, const int* br, const int* b
   const int block = 256;
   const unsigned grid = (unsigned)cdiv((long long)nbr * sw, block);
   switch (sw) {
-    case 1: bsr_kernel<1, BS, ROW0, VT, XT, Epi><<<grid, block, 0, st>>>(nbr, br, bc, bv, plane, x, epi); break;
-    case 2: bsr_kernel<2, BS, ROW0, VT, XT, Epi><<<grid, block, 0, st>>>(nbr, br, bc, bv, plane, x, epi); break;
-    case 4: bsr_kernel<4, BS, ROW0, VT, XT, Epi><<<grid, block, 0, st>>>(nbr, br, bc, bv, plane, x, epi); break;
-    case 8: bsr_kernel<8, BS, ROW0, VT, XT, Epi><<<grid, block, 0, st>>>(nbr, br, bc, bv, plane, x, epi); break;
-    default: bsr_kernel<16, BS, ROW0, VT, XT, Epi><<<grid, block, 0, st>>>(nbr, br, bc, bv, plane, x, epi); break;
+    case 1: launch_k(bsr_kernel<1, BS, ROW0, VT, XT, Epi>, grid, block, 0, st, nbr, br, bc, bv, plane, x, epi); break;
+    case 2: launch_k(bsr_kernel<2, BS, ROW0, VT, XT, Epi>, grid, block, 0, st, nbr, br, bc, bv, plane, x, epi); break;
+    case 4: launch_k(bsr_kernel<4, BS, ROW0, VT, XT, Epi>, grid, block, 0, st, nbr, br, bc, bv, plane, x, epi); break;
+    case 8: launch_k(bsr_kernel<8, BS, ROW0, VT, XT, Epi>, grid, block, 0, st, nbr, br, bc, bv, plane, x, epi); break;
+    default: launch_k(bsr_kernel<16, BS, ROW0, VT, XT, Epi>, grid, block, 0, st, nbr, br, bc, bv, plane, x, epi); break;
   }
   DECO_CHECK_LAUNCH();
 }
