@@ -609,7 +609,7 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots_reg(long long n, long l
 // could take more, the early SMs fill up and the grid's equal shares pile on
 // fewer SMs.  (Measured on the 1.5M-row system: the float32 dot pass with room
 // for three blocks per SM took 0.330 ms per iteration against 0.259 ms capped.)
-size_t smem_for_blocks(int blocks, size_t need, size_t static_bytes) {
+size_t smem_for_blocks(int blocks, size_t need) {
   static std::mutex mu;
   static std::vector<std::pair<int, int>> per_dev;  // (shared memory per SM, reserved per block)
   int dev = 0;
@@ -624,10 +624,12 @@ size_t smem_for_blocks(int blocks, size_t need, size_t static_bytes) {
     }
     a = per_dev[dev];
   }
-  const size_t sm = (size_t)a.first, res = (size_t)a.second + static_bytes;
-  size_t cap = sm / (blocks + 1) + 16 - res;  // blocks + 1 no longer fit
-  cap = (cap + 15) / 16 * 16;
-  if (need >= cap || (size_t)blocks * (cap + res) > sm) return need;
+  const size_t sm = (size_t)a.first, res = (size_t)a.second;
+  // blocks + 1 blocks would need more than the SM has, whatever the kernel's
+  // static shared memory and the allocation rounding; `blocks` still fit with
+  // up to 1 KB of static shared memory each
+  const size_t cap = (sm / (blocks + 1) + 15) / 16 * 16;
+  if (need >= cap || (size_t)blocks * (cap + res + 1024) > sm) return need;
   return cap;
 }
 
@@ -660,13 +662,12 @@ template <int CPW>
 void launch_dots_f32(cudaStream_t s, dim3 grid, size_t shm, long long n, long long ld, int nc, int j, const float* V,
                      const float* w, double* red, unsigned* counter, State st) {
   allow_dots_smem<CPW>();
-  constexpr size_t kStatic = 64;  // the kernels' static shared memory (last-block flag), rounded up
   if (CPW >= 4)
-    launch_k(arnoldi_dots_bulk<CPW>, grid, kThreads, smem_for_blocks(2, kDotsStageBytes + kDotsBarBytes + shm, kStatic),
-             s, n, ld, nc, j, V, w, red, counter, st);
+    launch_k(arnoldi_dots_bulk<CPW>, grid, kThreads, smem_for_blocks(2, kDotsStageBytes + kDotsBarBytes + shm), s, n,
+             ld, nc, j, V, w, red, counter, st);
   else
-    launch_k(arnoldi_dots<float, CPW>, grid, kThreads, smem_for_blocks(2, kDotsStageBytes + shm, kStatic), s, n, ld, nc,
-             j, V, w, red, counter, st);
+    launch_k(arnoldi_dots<float, CPW>, grid, kThreads, smem_for_blocks(2, kDotsStageBytes + shm), s, n, ld, nc, j, V, w,
+             red, counter, st);
 }
 
 template <typename T>
@@ -1059,7 +1060,7 @@ struct Solver {
     hs.tag = dtag + j % kRing;
     hs.t = tags[j % kRing] = g_step_tag.fetch_add(1, std::memory_order_relaxed) + 1;
     // nb = 4 blocks per SM (smem_for_blocks: no fifth block on an SM)
-    launch_k(arnoldi_update<T>, nb, kThreads, smem_for_blocks(4, sizeof(double) * 4 * (nc + 1), 128), s, n, ld, nc, j,
+    launch_k(arnoldi_update<T>, nb, kThreads, smem_for_blocks(4, sizeof(double) * 4 * (nc + 1)), s, n, ld, nc, j,
              V.get(), w.get(), col(j + 1), ctx->red.get(), ctx->counter.get(), st, hs);
     DECO_CHECK_LAUNCH();
     if (profile) DECO_CUDA(cudaEventRecord(pev[4 * j + 3], s));
