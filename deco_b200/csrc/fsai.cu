@@ -11,9 +11,11 @@
 // restatement bit for bit and the reference's LAPACK to rounding.
 //
 // Rows are grouped by order k into classes and processed in ONE launch:
-//   class 1 (1 <= k <= 8):  one thread per row, M held in registers;
-//   class 2 (8 < k <= 32):  one warp per row, M in shared memory;
-//   class 3 (32 < k <= 64): one warp per row, M in shared memory (32 KB).
+//   class 1 (k <= 8): one thread per row, M held in registers;
+//   classes 2-3 (k <= 16, <= 32): a group of S = 16 or 32 lanes per row, lane
+//            c holding column c of M in registers; the pivot row's multipliers
+//            travel by shuffles;
+//   class 4 (32 < k <= 64): one warp per row, M in shared memory (32 KB).
 #include <algorithm>
 
 #include <climits>
@@ -25,9 +27,7 @@ namespace deco {
 namespace {
 
 constexpr int kLuBlock = 128;
-constexpr int kRegK = 8;
-// per warp of class 2: 32x32 system + two rhs + pivots = 8832 B, four warps per block;
-// class 3: 64x64 system + rhs + pivots = 34048 B for the block's first warp
+// class 4: 64x64 system + rhs + pivots = 34048 B for the block's first warp
 constexpr int kSmemBytes = 36 * 1024;
 
 __device__ __forceinline__ int bsearch_le(const int* __restrict__ a, int lo, int hi, int target) {
@@ -163,11 +163,13 @@ __global__ void __launch_bounds__(kSqWarps * 32) lower_square(int n, const int* 
 }
 
 // ------------------------------------------------------------- row classes
-__device__ __forceinline__ int order_class(int k) { return k <= 0 ? 0 : (k <= kRegK ? 1 : (k <= 32 ? 2 : (k <= 64 ? 3 : 4))); }
+__device__ __forceinline__ int order_class(int k) {
+  return k <= 0 ? 0 : (k <= 8 ? 1 : (k <= 16 ? 2 : (k <= 32 ? 3 : (k <= 64 ? 4 : 5))));
+}
 
 __global__ void class_hist(int n, const int* __restrict__ fr, int* __restrict__ hist, int* __restrict__ kmax) {
-  __shared__ int h[5];
-  if (threadIdx.x < 5) h[threadIdx.x] = 0;
+  __shared__ int h[6];
+  if (threadIdx.x < 6) h[threadIdx.x] = 0;
   __syncthreads();
   int m = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -178,7 +180,7 @@ __global__ void class_hist(int n, const int* __restrict__ fr, int* __restrict__ 
   m = __reduce_max_sync(0xffffffffu, m);
   if ((threadIdx.x & 31) == 0) atomicMax(kmax, m);
   __syncthreads();
-  if (threadIdx.x < 5 && h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
+  if (threadIdx.x < 6 && h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
 }
 
 // warp-aggregated: lanes of one class share a single atomic on the class cursor
@@ -190,9 +192,9 @@ __global__ void class_scatter(int n, const int* __restrict__ fr, int* __restrict
     const unsigned same = __match_any_sync(0xffffffffu, cl);
     const int leader = __ffs(same) - 1;
     int pos = 0;
-    if (lane == leader && cl >= 1 && cl <= 3) pos = atomicAdd(&cursor[cl], __popc(same));
+    if (lane == leader && cl >= 1 && cl <= 4) pos = atomicAdd(&cursor[cl], __popc(same));
     pos = __shfl_sync(0xffffffffu, pos, leader) + __popc(same & ((1u << lane) - 1));
-    if (i < n && cl >= 1 && cl <= 3) perm[pos] = i;
+    if (i < n && cl >= 1 && cl <= 4) perm[pos] = i;
   }
 }
 
@@ -337,7 +339,147 @@ __device__ void solve_row_reg(int i, const int* __restrict__ Ar, const int* __re
     if (t < k) { FLv[a + t] = rl[t]; FUv[a + t] = ru[t]; }
 }
 
-// ------------------------------------------------- classes 2-3: warp per row
+// --------------------------------------- classes 2-3: a lane group per row
+// S lanes (16 or 32; k <= S) solve one row's system.  Lane c holds column c
+// of M in registers (col[t] = M(t, c)), ru_c and, as the factorisation moves
+// rows, the entry of rl at its current row position (rl is carried along with
+// the row swaps and eliminated step by step, which is the forward substitution
+// P M = L U needs).  Every element sees the separately rounded operations of the
+// textbook order the thread-per-row form used:
+//   step j: pivot = first index of the largest |M(x, j)|, x >= j (lane j scans
+//   its column); rows j and p swapped in every column; lane j scales its
+//   multipliers by 1 / M(j, j); the multipliers reach every lane by shuffles and
+//   column t subtracts M(x, j) M(j, t) from M(x, t); row x of rl subtracts
+//   M(x, j) rl_j;
+// then U^T a = ru (right-looking, lane j accumulating in ascending x), the
+// unit L^T sweep from the bottom (each b_j sums its terms in ascending x, so it
+// runs serially, lane j after lane j + 1), the pivots undone on b, and U on rl
+// from the bottom.  Loops run to S with predicates on k, so the two or four
+// groups of a warp stay converged for the full-warp shuffles.
+// Shared memory per group: the pattern (S ints), b (S doubles), pivots (S ints).
+template <int S>
+__device__ void solve_row_group(int i, int* __restrict__ sP, double* __restrict__ sb, int* __restrict__ spv,
+                                const int* __restrict__ Ar, const int* __restrict__ Ac, const double* __restrict__ Av,
+                                const int* __restrict__ Fr, const int* __restrict__ Fc, double* __restrict__ FLv,
+                                double* __restrict__ FUv) {
+  constexpr unsigned kAll = 0xffffffffu;
+  const int g = threadIdx.x & (S - 1);
+  int a = 0, k = 0, d = 0;
+  if (i >= 0) {
+    a = Fr[i];
+    const int e = Fr[i + 1] - 1;
+    k = e - a;
+    d = Fc[e];
+  }
+  if (g < k) sP[g] = Fc[a + g];
+  __syncwarp();
+  // gather: col[t] = M(t, g) = A(P[g], P[t]);  ru = -A(P[g], d);  rl = -A(d, P[g])
+  double col[S];
+#pragma unroll
+  for (int t = 0; t < S; ++t) col[t] = 0.0;
+  double ru = 0.0, rl = 0.0;
+  if (g < k) {
+    const int pg = sP[g];
+    const int ga = Ar[pg], gb = Ar[pg + 1];
+    int q = 0;  // merge pointer into the (ascending) pattern
+    for (int s2 = ga; s2 < gb; ++s2) {
+      const int cc = Ac[s2];
+      while (q < k && sP[q] < cc) ++q;
+      if (q < k && sP[q] == cc) {
+        const double val = Av[s2];
+#pragma unroll
+        for (int t = 0; t < S; ++t)
+          if (t == q) col[t] = val;
+      }
+      if (cc == d) ru = -Av[s2];
+    }
+    const int da = Ar[d], db = Ar[d + 1];
+    const int jx = bsearch_le(Ac, da, db, pg);
+    if (Ac[jx] == pg) rl = -Av[jx];
+  }
+  // LU with partial pivoting, rl carried along (forward substitution with unit L)
+#pragma unroll
+  for (int j = 0; j < S; ++j) {
+    int p = j;
+    if (g == j) {
+      double best = fabs(col[j]);
+#pragma unroll
+      for (int x = 0; x < S; ++x)
+        if (x > j && x < k && fabs(col[x]) > best) { best = fabs(col[x]); p = x; }
+    }
+    p = __shfl_sync(kAll, p, j, S);
+    if (g == 0) spv[j] = p;
+    if (p != j) {  // uniform over the group
+#pragma unroll
+      for (int x = 0; x < S; ++x)
+        if (x > j && x == p) { const double t = col[j]; col[j] = col[x]; col[x] = t; }
+    }
+    {
+      const double rj = __shfl_sync(kAll, rl, j, S), rp = __shfl_sync(kAll, rl, p, S);
+      if (g == j) rl = rp;
+      else if (g == p) rl = rj;
+    }
+    if (g == j && j < k && col[j] != 0.0) {
+      const double inv = __ddiv_rn(1.0, col[j]);
+#pragma unroll
+      for (int x = 0; x < S; ++x)
+        if (x > j && x < k) col[x] = __dmul_rn(col[x], inv);
+    }
+    const double rlj = __shfl_sync(kAll, rl, j, S);
+#pragma unroll
+    for (int x = 0; x < S; ++x) {
+      if (x <= j) continue;  // (constant bounds: every loop here unrolls to static register indices)
+      const double mx = __shfl_sync(kAll, col[x], j, S);  // M(x, j), the multiplier
+      if (x < k) {
+        if (g > j && g < k) col[x] = msub(col[x], mx, col[j]);
+        if (g == x) rl = msub(rl, mx, rlj);
+      }
+    }
+  }
+  // U^T a = ru: lane g holds s_g; a_x = s_x / U(x, x), then s_g -= U(x, g) a_x for g > x
+#pragma unroll
+  for (int x = 0; x < S; ++x) {
+    if (g == x && x < k) ru = __ddiv_rn(ru, col[x]);
+    const double ax = __shfl_sync(kAll, ru, x, S);
+    if (g > x && g < k && x < k) ru = msub(ru, col[x], ax);
+  }
+  // unit L^T b = a from the bottom: b_j = a_j - sum_{x > j} L(x, j) b_x, x ascending
+#pragma unroll
+  for (int j = S - 1; j >= 0; --j) {
+    if (g == j && j < k) {
+      double s2 = ru;
+#pragma unroll
+      for (int x = 0; x < S; ++x)
+        if (x > j && x < k) s2 = msub(s2, col[x], sb[x]);
+      sb[j] = s2;
+    }
+    __syncwarp();
+  }
+  // fU = P^T b
+  if (g == 0)
+    for (int j = k - 1; j >= 0; --j) {
+      const int pj = spv[j];
+      if (pj != j) { const double t = sb[j]; sb[j] = sb[pj]; sb[pj] = t; }
+    }
+  __syncwarp();
+  if (g < k) FUv[a + g] = sb[g];
+  // U fL = (L^-1 P rl) from the bottom: rl_j /= U(j, j), then rl_x -= U(x, j) rl_j for x < j
+#pragma unroll
+  for (int j = S - 1; j >= 0; --j) {
+    if (g == j && j < k) rl = __ddiv_rn(rl, col[j]);
+    const double rj = __shfl_sync(kAll, rl, j, S);
+#pragma unroll
+    for (int x = 0; x < S; ++x) {
+      if (x >= j) continue;
+      const double ux = __shfl_sync(kAll, col[x], j, S);  // U(x, j) from lane j
+      if (g == x && j < k) rl = msub(rl, ux, rj);
+    }
+  }
+  if (g < k) FLv[a + g] = rl;
+  __syncwarp();
+}
+
+// --------------------------------------------------- class 4: warp per row
 // M column-major in shared memory: M(i,j) = sm[i + j*k].
 __device__ int find_in_pattern(const int* __restrict__ P, int k, int key) {
   int lo = 0, hi = k - 1;
@@ -449,34 +591,48 @@ __device__ void solve_row_warp(int i, double* __restrict__ sm, double* __restric
   __syncwarp();
 }
 
-// one launch: blocks [0,b1) class 1, [b1,b1+b2) class 2, then class 3
+// one launch: blocks [0,b1) class 1 (a row per thread), [b1,b2) class 2 (8 per
+// block), [b2,b3) class 3 (4 per block), then class 4 (one per block); perm holds
+// the rows class by class, from offsets o[0..3]
+template <int S>
+__device__ __forceinline__ void group_row(int q, int nq, const int* __restrict__ rows, int* gP, double* gB, int* gPv,
+                                          const int* __restrict__ Ar, const int* __restrict__ Ac,
+                                          const double* __restrict__ Av, const int* __restrict__ Fr,
+                                          const int* __restrict__ Fc, double* __restrict__ FLv,
+                                          double* __restrict__ FUv) {
+  const int g0 = threadIdx.x & ~(S - 1);  // the group's first thread: its slice of the shared arrays
+  solve_row_group<S>(q < nq ? rows[q] : -1, gP + g0, gB + g0, gPv + g0, Ar, Ac, Av, Fr, Fc, FLv, FUv);
+}
+
 __global__ void __launch_bounds__(kLuBlock) fsai_local_systems(
-    const int* __restrict__ perm, int n1, int n2, int n3, int b1, int b2, const int* __restrict__ Ar,
+    const int* __restrict__ perm, int4 cnt, int4 off, int b1, int b2, int b3, const int* __restrict__ Ar,
     const int* __restrict__ Ac, const double* __restrict__ Av, const int* __restrict__ Fr,
     const int* __restrict__ Fc, double* __restrict__ FLv, double* __restrict__ FUv) {
   extern __shared__ double smem[];
+  __shared__ int gP[kLuBlock];
+  __shared__ double gB[kLuBlock];
+  __shared__ int gPv[kLuBlock];
   const int b = blockIdx.x;
   if (b < b1) {
     const int q = b * kLuBlock + threadIdx.x;
-    if (q < n1) solve_row_reg<kRegK>(perm[q], Ar, Ac, Av, Fr, Fc, FLv, FUv);
+    if (q < cnt.x) solve_row_reg<8>(perm[off.x + q], Ar, Ac, Av, Fr, Fc, FLv, FUv);
     return;
   }
-  const int warp = threadIdx.x >> 5;
-  if (b < b1 + b2) {
-    const int q = (b - b1) * (kLuBlock / 32) + warp;
-    if (q >= n2) return;
-    // per warp: 32x32 system + rhs + pivots
-    double* base = smem + warp * (32 * 32 + 64 + 16);
-    solve_row_warp(perm[n1 + q], base, base + 32 * 32, base + 32 * 32 + 32, reinterpret_cast<int*>(base + 32 * 32 + 64),
-                   Ar, Ac, Av, Fr, Fc, FLv, FUv);
+  if (b < b2) {
+    group_row<16>((b - b1) * (kLuBlock / 16) + threadIdx.x / 16, cnt.y, perm + off.y, gP, gB, gPv, Ar, Ac, Av, Fr,
+                  Fc, FLv, FUv);
     return;
   }
-  const int q = b - b1 - b2;
-  if (warp != 0 || q >= n3) return;
+  if (b < b3) {
+    group_row<32>((b - b2) * (kLuBlock / 32) + threadIdx.x / 32, cnt.z, perm + off.z, gP, gB, gPv, Ar, Ac, Av, Fr,
+                  Fc, FLv, FUv);
+    return;
+  }
+  const int q = b - b3;
+  if ((threadIdx.x >> 5) != 0 || q >= cnt.w) return;
   double* base = smem;  // 64x64 system (32 KB), then rhs and pivots
   double* rl = smem + 64 * 64;
-  solve_row_warp(perm[n1 + n2 + q], base, rl, rl + 64, reinterpret_cast<int*>(rl + 128), Ar, Ac, Av, Fr, Fc, FLv,
-                 FUv);
+  solve_row_warp(perm[off.w + q], base, rl, rl + 64, reinterpret_cast<int*>(rl + 128), Ar, Ac, Av, Fr, Fc, FLv, FUv);
 }
 
 // ------------------------------------------------- D-scaling (diagonal.cpp)
@@ -678,23 +834,27 @@ void fsai_build(deco_ctx_s* ctx, const deco_csr_s* A0, double tol_rel, double to
   DECO_CUDA(cudaMemcpyAsync(h, hist.get(), sizeof(h), cudaMemcpyDeviceToHost, st));
   DECO_CUDA(cudaStreamSynchronize(st));
   F->max_order = h[8];
-  DECO_REQUIRE(h[4] == 0, DECO_ERR_UNSUPPORTED,
+  DECO_REQUIRE(h[5] == 0, DECO_ERR_UNSUPPORTED,
                "FSAI local system of order " + std::to_string(h[8]) + " exceeds the supported maximum of 64");
-  const int n1 = h[1], n2 = h[2], n3 = h[3];
-  const int nsolve = n1 + n2 + n3;
+  const int n1 = h[1], n2 = h[2], n3 = h[3], n4 = h[4];
+  const int nsolve = n1 + n2 + n3 + n4;
   if (nsolve > 0) {
     DevBuf<int> perm(nsolve, st);
-    int cur[4] = {0, 0, n1, n1 + n2};
-    DevBuf<int> cursor(4, st);
+    int cur[5] = {0, 0, n1, n1 + n2, n1 + n2 + n3};
+    DevBuf<int> cursor(5, st);
     DECO_CUDA(cudaMemcpyAsync(cursor.get(), cur, sizeof(cur), cudaMemcpyHostToDevice, st));
     class_scatter<<<g, 256, 0, st>>>(n, FL.r.get(), cursor.get(), perm.get());
     DECO_CHECK_LAUNCH();
-    const int b1 = (int)cdiv(n1, kLuBlock), b2 = (int)cdiv(n2, kLuBlock / 32), b3 = n3;
-    const size_t smem = (n2 + n3) > 0 ? kSmemBytes : 0;
+    const int b1 = (int)cdiv(n1, kLuBlock);
+    const int b2 = b1 + (int)cdiv(n2, kLuBlock / 16);
+    const int b3 = b2 + (int)cdiv(n3, kLuBlock / 32);
+    const int nblk = b3 + n4;
+    const size_t smem = n4 > 0 ? kSmemBytes : 0;
     if (smem) DECO_CUDA(cudaFuncSetAttribute(fsai_local_systems, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
-    fsai_local_systems<<<b1 + b2 + b3, kLuBlock, smem, st>>>(perm.get(), n1, n2, n3, b1, b2, A->r.get(),
-                                                                A->c.get(), A->v.get(), FL.r.get(), FL.c.get(),
-                                                                FL.v.get(), fu.get());
+    fsai_local_systems<<<nblk, kLuBlock, smem, st>>>(perm.get(), make_int4(n1, n2, n3, n4),
+                                                      make_int4(0, n1, n1 + n2, n1 + n2 + n3), b1, b2, b3,
+                                                      A->r.get(), A->c.get(), A->v.get(), FL.r.get(), FL.c.get(),
+                                                      FL.v.get(), fu.get());
     DECO_CHECK_LAUNCH();
   }
   trace_mark(ctx, "fsai local systems");

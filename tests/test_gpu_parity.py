@@ -206,6 +206,33 @@ def test_cpr_setup_and_apply(d, oracle, name, case):
 
 
 @pytest.mark.parametrize("name", ["c1", "bs3_faults"])
+@pytest.mark.parametrize("power", [1, 2])
+def test_fsai_local_systems_bit_exact_vs_oracle(d, oracle, name, power):
+    """The batched local solves follow the oracle's textbook LU with partial
+    pivoting operation by operation, in every order class (8, 16 and 32 lanes per
+    row, and one warp per row past order 32): both FSAI factors of a CPR setup
+    equal the C restatement's bit for bit."""
+    port, _ = oracle
+    s = system(name)
+    prec = cpr_json(s.bs, glo_power=power, loc_power=power)
+    A = d.CSR.from_system(s)
+    P = d.CPR(prec, A, cuda(s.b))
+    O = port.Cpr(prec, s.r, s.c, s.v, s.b)
+    orders = []
+    for which in (0, 1):
+        (Lr, Lc, Lv), (Ur, Uc, Uv) = P.fsai(which).factors()
+        (OLr, OLc, OLv), (OUr, OUc, OUv) = O.fsai(which)
+        np.testing.assert_array_equal(Lc, OLc)
+        np.testing.assert_array_equal(Uc, OUc)
+        np.testing.assert_array_equal(Lv, OLv)
+        np.testing.assert_array_equal(Uv, OUv)
+        orders.append(np.diff(Lr) - 1)
+    k = np.concatenate(orders)
+    print(f"{name} power {power}: local orders {k.min()}..{k.max()}, "
+          f"rows per class (<=8, <=16, <=32, <=64): {[(k <= 8).sum(), ((k > 8) & (k <= 16)).sum(), ((k > 16) & (k <= 32)).sum(), (k > 32).sum()]}")
+
+
+@pytest.mark.parametrize("name", ["c1", "bs3_faults"])
 @pytest.mark.parametrize("weights", ["quasiimpes", "none"])
 def test_cpr_pressure_id_1_matches_reference(d, oracle, name, weights):
     """pressure_id 1 (CPR.hpp:50): the quasi-IMPES weights solve B^T w = e_1 (CPR.hpp:336),
