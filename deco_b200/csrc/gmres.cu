@@ -706,12 +706,25 @@ __global__ void __launch_bounds__(kThreads) arnoldi_update(long long n, long lon
   constexpr int N = Vec4<T>::N;
   constexpr int U = N == 4 ? 16 : 8;
   extern __shared__ double dyn_u[];
+  const long long nvec = n / N;
+  // Before the dependency wait: L2 prefetches of this thread's first vector of w
+  // and of up to U basis columns (written two or more kernels back; only the
+  // coefficients come from the dot pass), so that DRAM traffic overlaps the dot
+  // pass's last block forming the coefficients.  No registers are held.
+  {
+    const long long v0 = (long long)blockIdx.x * kThreads + threadIdx.x;
+    if (v0 < nvec) {
+      asm volatile("prefetch.global.L2 [%0];\n" ::"l"(reinterpret_cast<const VT*>(w) + v0));
+      const int np = ncols < U ? ncols : U;
+      for (int u = 0; u < np; ++u)
+        asm volatile("prefetch.global.L2 [%0];\n" ::"l"(reinterpret_cast<const VT*>(V + (size_t)u * ld) + v0));
+    }
+  }
   pdl_wait();
   pdl_trigger();
   double* cs_ = dyn_u;
   for (int i = threadIdx.x; i < ncols; i += kThreads) cs_[i] = st.c[i];
   __syncthreads();
-  const long long nvec = n / N;
   double ss = 0.0;
   for (long long vi = (long long)blockIdx.x * kThreads + threadIdx.x; vi < nvec;
        vi += (long long)gridDim.x * kThreads) {
