@@ -89,6 +89,61 @@ __global__ void ell2_fill(int nbr, int W, const int* __restrict__ br, const int*
   }
 }
 
+// blocks-per-cell histogram (cells with kHistCap or more blocks counted together)
+constexpr int kHistCap = 32;
+__global__ void block_hist(const int* __restrict__ br, int nbr, int* __restrict__ hist) {
+  __shared__ int h[kHistCap + 1];
+  for (int t = threadIdx.x; t <= kHistCap; t += blockDim.x) h[t] = 0;
+  __syncthreads();
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nbr; s += gridDim.x * blockDim.x)
+    atomicAdd(&h[min(br[s + 1] - br[s], kHistCap)], 1);
+  __syncthreads();
+  for (int t = threadIdx.x; t <= kHistCap; t += blockDim.x)
+    if (h[t]) atomicAdd(&hist[t], h[t]);
+}
+
+// blocks of cell s past its first W - 1 when it has more than W (0 otherwise)
+__global__ void overflow_count(const int* __restrict__ br, int nbr, int W, int* __restrict__ cnt) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nbr; s += gridDim.x * blockDim.x) {
+    const int nb = br[s + 1] - br[s];
+    cnt[s] = nb > W ? nb - (W - 1) : 0;
+  }
+}
+
+template <typename T> __device__ __forceinline__ T int_bits(int v);
+template <> __device__ __forceinline__ double int_bits<double>(int v) { return __longlong_as_double((long long)v); }
+template <> __device__ __forceinline__ float int_bits<float>(int v) { return __int_as_float(v); }
+
+// slot-major padded 3x3 cells (columns too when ec != nullptr) and the overflow
+// list of the cells wider than W (from ostart, the scan of overflow_count)
+template <typename T>
+__global__ void ell3_fill(int nbr, int W, const int* __restrict__ br, const int* __restrict__ bc,
+                          const T* __restrict__ bv, long long plane, const int* __restrict__ ostart,
+                          int* __restrict__ ec, T* __restrict__ ev, int* __restrict__ oc, T* __restrict__ ov) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nbr; s += gridDim.x * blockDim.x) {
+    const int a = br[s], e = br[s + 1], nb = e - a;
+    const bool over = nb > W;
+    for (int k = 0; k < W; ++k) {
+      const bool mark = over && k == W - 1;
+      const bool on = !mark && a + k < e;
+      // an unused slot reads a column the cell already has (or column 0) with zero values
+      if (ec) ec[(long long)k * nbr + s] = mark ? -1 : (on ? bc[a + k] : (e > a ? bc[a] : 0));
+      for (int p = 0; p < 9; ++p) {
+        T val = on ? bv[(p / 3) * plane + 3LL * (a + k) + p % 3] : (T)0;
+        if (mark && p == 0) val = int_bits<T>(ostart[s]);
+        if (mark && p == 1) val = int_bits<T>(nb - (W - 1));
+        ev[((long long)p * W + k) * nbr + s] = val;
+      }
+    }
+    if (over)
+      for (int i = 0; i < nb - (W - 1); ++i) {
+        const int blk = a + W - 1 + i, o = ostart[s] + i;
+        if (oc) oc[o] = bc[blk];
+        for (int p = 0; p < 9; ++p) ov[9LL * o + p] = bv[(p / 3) * plane + 3LL * blk + p % 3];
+      }
+  }
+}
+
 // ---- offset-coded slot columns
 // The distinct column offsets of the slots (column minus the slot's own row or
 // cell) go into an open-addressing set of kSetCap entries; when more than
@@ -190,7 +245,58 @@ void make_slot_codes(deco_ctx_s* ctx, deco_csr_s* A, int nrow) {
   DECO_CUDA(cudaStreamSynchronize(st));  // `off` (host) must outlive the copy
 }
 
+void make_padded3(deco_ctx_s* ctx, deco_csr_s* A) {
+  cudaStream_t st = ctx->stream;
+  const int nbr = A->n / 3;
+  if (!A->ew) {
+    if (!ctx->padded || nbr <= 0 || A->m < 3) return;
+    DevBuf<int> hist(kHistCap + 1, st);
+    hist.zero(st);
+    block_hist<<<grid_for(ctx, nbr, 256), 256, 0, st>>>(A->br.get(), nbr, hist.get());
+    DECO_CHECK_LAUNCH();
+    std::vector<int> h(kHistCap + 1);
+    DECO_CUDA(cudaMemcpyAsync(h.data(), hist.get(), sizeof(int) * h.size(), cudaMemcpyDeviceToHost, st));
+    DECO_CUDA(cudaStreamSynchronize(st));
+    // the fewest slots (4, 7 or 8) that leave at most 2 % of the cells to the
+    // overflow list and pad at most 25 % over the blocks stored
+    int W = 0;
+    for (int cand : {4, 7, 8}) {
+      long long over = 0;
+      for (int b = cand + 1; b <= kHistCap; ++b) over += h[b];
+      if (over <= nbr / 50 && (double)cand * nbr <= 1.25 * A->nblk && h[kHistCap] == 0) { W = cand; break; }
+    }
+    if (!W) return;
+    DevBuf<int> cnt(nbr + 1, st), ostart(nbr + 1, st);
+    overflow_count<<<grid_for(ctx, nbr, 256), 256, 0, st>>>(A->br.get(), nbr, W, cnt.get());
+    DECO_CHECK_LAUNCH();
+    A->nov = (int)exclusive_scan_int(ctx, cnt.get(), ostart.get(), nbr);
+    A->ew = W;
+    A->ec.alloc((size_t)W * nbr, st);
+    A->ev.alloc((size_t)9 * W * nbr, st);
+    A->oc.alloc(std::max(A->nov, 1), st);
+    A->ov.alloc((size_t)9 * std::max(A->nov, 1), st);
+    A->eo = std::move(ostart);
+    ell3_fill<double><<<grid_for(ctx, nbr, 256), 256, 0, st>>>(nbr, W, A->br.get(), A->bc.get(), A->bv.get(),
+                                                               A->bplane, A->eo.get(), A->ec.get(), A->ev.get(),
+                                                               A->oc.get(), A->ov.get());
+    DECO_CHECK_LAUNCH();
+  }
+  if (A->bv32) {
+    const int W = A->ew;
+    if (!A->ev32 || A->ev32.size() != (size_t)9 * W * nbr) A->ev32.alloc((size_t)9 * W * nbr, st);
+    if (!A->ov32 || A->ov32.size() != (size_t)9 * std::max(A->nov, 1)) A->ov32.alloc((size_t)9 * std::max(A->nov, 1), st);
+    ell3_fill<float><<<grid_for(ctx, nbr, 256), 256, 0, st>>>(nbr, W, A->br.get(), A->bc.get(), A->bv32.get(),
+                                                              A->bplane, A->eo.get(), nullptr, A->ev32.get(), nullptr,
+                                                              A->ov32.get());
+    DECO_CHECK_LAUNCH();
+  }
+}
+
 void make_padded(deco_ctx_s* ctx, deco_csr_s* A) {
+  if (A->bbs == 3) {
+    make_padded3(ctx, A);
+    return;
+  }
   cudaStream_t st = ctx->stream;
   const int nbr = A->n / 2;
   if (!A->ew) {
@@ -281,6 +387,11 @@ void drop_bsr(deco_csr_s* A) {
   A->eb = A->noff = 0;
   A->ecode = DevBuf<unsigned char>();
   A->eoff = DevBuf<int>();
+  A->nov = 0;
+  A->oc = DevBuf<int>();
+  A->ov = DevBuf<double>();
+  A->ov32 = DevBuf<float>();
+  A->eo = DevBuf<int>();
 }
 
 void make_bsr(deco_ctx_s* ctx, deco_csr_s* A, int bs, double max_fill) {
@@ -411,7 +522,7 @@ int tuned_bsr_subwarp(deco_ctx_s* ctx, deco_csr_s* A, bool f32) {
 void tune_product_plan(deco_ctx_s* ctx, deco_csr_s* A, bool f32) {
   int& plan = f32 ? A->plan32 : A->plan64;
   if (plan || !ctx->autotune || A->n < 4096 || (f32 && !A->v32)) return;
-  const bool ell = A->ew && (!f32 || A->ev32) && (A->bbs == 2 || A->bbs == 0);
+  const bool ell = A->ew && (!f32 || A->ev32);
   const bool cells = A->bbs > 1 && (!f32 || A->bv32);
   const int first = ell ? 1 : (cells ? 2 : 3);  // what the layout rules pick
   if (!ell && !cells) return;                    // CSR is the only product
@@ -435,13 +546,13 @@ void tune_product_plan(deco_ctx_s* ctx, deco_csr_s* A, bool f32) {
   if (f32) { xf.alloc(A->m, ctx->stream); yf.alloc(A->n, ctx->stream); xf.zero(ctx->stream); }
   auto run = [&](int cand) {
     if (f32) {
-      if (cand == 1 && A->bbs) launch_ell2<float, float>(ctx->stream, A, false, xf.get(), EpiStore<float>{yf.get()});
+      if (cand == 1 && A->bbs) launch_ell_cells<float, float>(ctx->stream, A, false, xf.get(), EpiStore<float>{yf.get()});
       else if (cand == 1) launch_ell1<float, float>(ctx->stream, A, xf.get(), EpiStore<float>{yf.get()});
       else if (cand == 2) launch_bsr<float, float>(ctx->stream, A, bsw, false, xf.get(), EpiStore<float>{yf.get()});
       else launch_spmv_sw<float, float>(ctx->stream, csw, A->n, 1, A->r.get(), A->c.get(), A->v32.get(), xf.get(),
                                           EpiStore<float>{yf.get()});
     } else {
-      if (cand == 1 && A->bbs) launch_ell2<double, double>(ctx->stream, A, false, x.get(), EpiStore<double>{y.get()});
+      if (cand == 1 && A->bbs) launch_ell_cells<double, double>(ctx->stream, A, false, x.get(), EpiStore<double>{y.get()});
       else if (cand == 1) launch_ell1<double, double>(ctx->stream, A, x.get(), EpiStore<double>{y.get()});
       else if (cand == 2) launch_bsr<double, double>(ctx->stream, A, bsw, false, x.get(), EpiStore<double>{y.get()});
       else launch_spmv_sw<double, double>(ctx->stream, csw, A->n, 1, A->r.get(), A->c.get(), A->v.get(), x.get(),

@@ -90,6 +90,10 @@ void product_no_alloc(deco_ctx_s* ctx, deco_csr_s* A, const XT* x, Epi epi) {
       launch_ell2<VT, XT, Epi>(ctx->stream, A, false, x, epi);
       return;
     }
+    if (A->bbs == 3) {
+      launch_ell3<VT, XT, Epi>(ctx->stream, A, false, x, epi);
+      return;
+    }
   }
   const VT* v;
   if constexpr (sizeof(VT) == 4) v = A->v32.get(); else v = A->v.get();

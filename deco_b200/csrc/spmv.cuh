@@ -53,6 +53,17 @@ struct deco_csr_s {
   deco::DevBuf<int> ec;
   deco::DevBuf<double> ev;
   deco::DevBuf<float> ev32;
+  // 3x3 cell blocks (bbs == 3): ew slots per cell hold the cell's first blocks;
+  // a cell with more than ew blocks keeps ew - 1 in slots and marks the last
+  // slot with column -1, whose value planes 0 and 1 carry (as int bits) the
+  // start and count of its remaining blocks in the overflow list (oc: block
+  // columns; ov / ov32: the 9 values of each block, row-major).  Value plane
+  // 3 q + t of slot k (in-block row q, column t): ev[((3 q + t) ew + k) ncell + s].
+  int nov = 0;
+  deco::DevBuf<int> eo;  // per cell: start of its overflow blocks (the float32 refill reuses it)
+  deco::DevBuf<int> oc;
+  deco::DevBuf<double> ov;
+  deco::DevBuf<float> ov32;
   // Offset-coded slot columns: when the slots' column offsets (block column
   // minus the cell's own index, or column minus the row for scalar rows) take at
   // most 256 (eb = 1) or 65536 (eb = 2) distinct values, eoff holds them sorted
@@ -439,6 +450,94 @@ __global__ void __launch_bounds__(256) ell2_kernel(int nbr, const int* __restric
   }
 }
 
+// Slot-padded 3x3 product: one thread per cell, W slots, every value load a
+// coalesced 4- or 8-byte load of one of the 9 (3 for ROW0) slot-major value
+// planes; the block rows sum in slot order, which is the cell's block order
+// (as the cell-block kernel with one lane per cell sums them).  A slot with
+// column -1 (only the last) sends the thread to the cell's overflow blocks.
+template <typename VT> __device__ __forceinline__ int slot_bits(VT v);
+template <> __device__ __forceinline__ int slot_bits<double>(double v) { return (int)__double_as_longlong(v); }
+template <> __device__ __forceinline__ int slot_bits<float>(float v) { return __float_as_int(v); }
+
+template <bool ROW0, typename VT, typename XT>
+__device__ __forceinline__ void block3_accumulate(const VT (&w)[9], const XT* __restrict__ x, int col, double* sum) {
+  constexpr int NR = ROW0 ? 1 : 3;
+  using XA = typename std::conditional<kRunF32<VT, XT>, float, double>::type;
+  const long long j = 3LL * col;
+  XA xv[3];
+#pragma unroll
+  for (int t = 0; t < 3; ++t) xv[t] = (XA)__ldg(x + j + t);
+#pragma unroll
+  for (int q = 0; q < NR; ++q) {
+    if constexpr (kRunF32<VT, XT>) {
+      float run = w[3 * q] * xv[0];
+      run = fmaf(w[3 * q + 1], xv[1], run);
+      run = fmaf(w[3 * q + 2], xv[2], run);
+      sum[q] += (double)run;
+    } else {
+#pragma unroll
+      for (int t = 0; t < 3; ++t) sum[q] += (XA)w[3 * q + t] * xv[t];
+    }
+  }
+}
+
+template <int W, bool ROW0, typename VT, typename XT, class Epi>
+__global__ void __launch_bounds__(256) ell3_kernel(int nbr, const int* __restrict__ ec, const VT* __restrict__ ev,
+                                                   const int* __restrict__ oc, const VT* __restrict__ ov,
+                                                   const XT* __restrict__ x, Epi epi) {
+  constexpr int NR = ROW0 ? 1 : 3;
+  // float32 values: every slot's values are loaded up front (W x 3 NR registers),
+  // so a thread has all its matrix bytes in flight at once; float64 values are
+  // loaded slot by slot
+  constexpr bool kAll = sizeof(VT) == 4;
+  constexpr int WP = kAll ? W : 1;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nbr) return;
+  int cc[W];
+  VT wa[WP][3 * NR];
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    cc[k] = __ldcs(ec + (long long)k * nbr + s);
+    if constexpr (kAll) {
+#pragma unroll
+      for (int p = 0; p < 3 * NR; ++p) wa[k][p] = __ldcs(ev + ((long long)p * W + k) * nbr + s);
+    }
+  }
+  // the slots above are constant during a solve; x and the epilogue's vectors
+  // may be the predecessor's output
+  pdl_wait();
+  pdl_trigger();
+  double sum[NR];
+#pragma unroll
+  for (int q = 0; q < NR; ++q) sum[q] = 0.0;
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    VT w[9];
+#pragma unroll
+    for (int p = 0; p < 3 * NR; ++p) {
+      if constexpr (kAll) w[p] = wa[k][p];
+      else w[p] = __ldcs(ev + ((long long)p * W + k) * nbr + s);
+    }
+    if (k == W - 1 && cc[k] < 0) {  // the cell's remaining blocks, from the overflow list
+      const int o0 = slot_bits<VT>(w[0]), no = slot_bits<VT>(w[1]);
+      for (int o = o0; o < o0 + no; ++o) {
+        VT u[9];
+#pragma unroll
+        for (int p = 0; p < 9; ++p) u[p] = ov[9LL * o + p];
+        block3_accumulate<ROW0, VT, XT>(u, x, oc[o], sum);
+      }
+    } else {
+      block3_accumulate<ROW0, VT, XT>(w, x, cc[k], sum);
+    }
+  }
+  if (ROW0) {
+    epi(s, sum[0]);
+  } else {
+#pragma unroll
+    for (int q = 0; q < NR; ++q) epi(3 * s + q, sum[q]);
+  }
+}
+
 // Slot-padded scalar product (a CSR matrix with at most W entries per row: the
 // FSAI factors of a pressure system): one thread per row, slot-major coalesced
 // loads.  Float32 values times float32 x: each group of four slots is summed in
@@ -522,6 +621,32 @@ void launch_ell2(cudaStream_t st, const deco_csr_s* A, bool row0, const XT* x, E
   DECO_CHECK_LAUNCH();
 }
 
+template <typename VT, typename XT, class Epi>
+void launch_ell3(cudaStream_t st, const deco_csr_s* A, bool row0, const XT* x, Epi epi) {
+  const int nbr = A->n / 3;
+  if (nbr <= 0) return;
+  const VT* ev;
+  const VT* ov;
+  if constexpr (sizeof(VT) == 4) { ev = A->ev32.get(); ov = A->ov32.get(); } else { ev = A->ev.get(); ov = A->ov.get(); }
+  const unsigned grid = (unsigned)cdiv(nbr, 256);
+  auto go = [&](auto wc) {
+    constexpr int W = decltype(wc)::value;
+    if (row0) launch_k(ell3_kernel<W, true, VT, XT, Epi>, grid, 256, 0, st, nbr, A->ec.get(), ev, A->oc.get(), ov, x, epi);
+    else launch_k(ell3_kernel<W, false, VT, XT, Epi>, grid, 256, 0, st, nbr, A->ec.get(), ev, A->oc.get(), ov, x, epi);
+  };
+  if (A->ew == 4) go(std::integral_constant<int, 4>{});
+  else if (A->ew == 7) go(std::integral_constant<int, 7>{});
+  else go(std::integral_constant<int, 8>{});
+  DECO_CHECK_LAUNCH();
+}
+
+// the slot-padded product of a cell-block matrix (2x2 or 3x3 cells)
+template <typename VT, typename XT, class Epi>
+void launch_ell_cells(cudaStream_t st, const deco_csr_s* A, bool row0, const XT* x, Epi epi) {
+  if (A->bbs == 3) launch_ell3<VT, XT, Epi>(st, A, row0, x, epi);
+  else launch_ell2<VT, XT, Epi>(st, A, row0, x, epi);
+}
+
 template <int BS, bool ROW0, typename VT, typename XT, class Epi>
 void launch_bsr_bs(cudaStream_t st, int sw, int nbr, const int* br, const int* bc, const VT* bv, long long plane,
                    const XT* x, Epi epi) {
@@ -599,7 +724,9 @@ void make_bsr(deco_ctx_s* ctx, deco_csr_s* A, int bs, double max_fill = 1.25);
 // Builds the slot-padded copy of a 2x2-block matrix (4 slots when no cell has
 // more than 4 blocks, else 7 or 8, the fewest that hold the widest cell, when the
 // padding stays within 25 %; otherwise none), float32 values too when the block
-// copy has them.
+// copy has them.  3x3-block matrices get 4, 7 or 8 slots, the fewest that hold
+// all but at most 2 % of the cells within 25 % padding, the rest of the wider
+// cells' blocks going to the overflow list.
 // make_bsr and make_f32_values call it.
 void make_padded(deco_ctx_s* ctx, deco_csr_s* A);
 // The scalar slot-padded copy of a CSR matrix without cell blocks (4 slots when no
@@ -623,7 +750,7 @@ void spmv(deco_ctx_s* ctx, deco_csr_s* A, const XT* x, Epi epi, int bs = 1) {
   if (plan != 3 && A->bbs > 1 && (bs == 1 || bs == A->bbs) && (!f32 || A->bv32) &&
       (reinterpret_cast<uintptr_t>(x) % (A->bbs == 2 ? 2 * sizeof(XT) : sizeof(XT))) == 0) {
     if (plan != 2 && A->ew && (!f32 || A->ev32)) {
-      launch_ell2<VT, XT, Epi>(ctx->stream, A, bs != 1, x, epi);
+      launch_ell_cells<VT, XT, Epi>(ctx->stream, A, bs != 1, x, epi);
       return;
     }
     launch_bsr<VT, XT, Epi>(ctx->stream, A, tuned_bsr_subwarp(ctx, A, f32), bs != 1, x, epi);

@@ -36,6 +36,25 @@ SYSTEMS = {
 }
 
 
+def blocks_per_cell(r, c, bs):
+    n = len(r) - 1
+    cells = np.repeat(np.arange(n) // bs, np.diff(r))
+    ncell = n // bs
+    u = np.unique(cells.astype(np.int64) * (c.max() // bs + 1) + c // bs)
+    return np.bincount(u // (c.max() // bs + 1), minlength=ncell)
+
+
+def expected_slots(s, bs, nblk):
+    ncell = s.n // bs
+    if bs == 2:
+        return 7 if 7 * ncell <= 1.25 * nblk else 0
+    cnt = blocks_per_cell(s.r, s.c, bs)
+    for w in (4, 7, 8):
+        if (cnt > w).sum() <= ncell // 50 and w * ncell <= 1.25 * nblk:
+            return w
+    return 0
+
+
 @pytest.mark.parametrize("name", list(SYSTEMS))
 def test_block_products_match_oracle(d, name):
     from oracle import port
@@ -44,8 +63,10 @@ def test_block_products_match_oracle(d, name):
     A.set_blocks(s.bs)
     bs, nblk = A.blocks
     assert bs == s.bs and nblk * bs * bs == s.nnz  # generated systems are dense cell blocks
-    # 7-point cells carry up to 7 blocks: 7 padded slots when that pads at most 25 %
-    assert A.padded == (7 if bs == 2 and 7 * (s.n // 2) <= 1.25 * nblk else 0)
+    # 7-point cells carry up to 7 blocks: 7 padded slots when that pads at most 25 %;
+    # 3x3 cells take the fewest of 4, 7, 8 slots that leave at most 2 % of the cells
+    # to the overflow list within 25 % padding
+    assert A.padded == expected_slots(s, bs, nblk)
     x = np.random.default_rng(0).standard_normal(s.n)
     assert rel(A.apply(cuda(x)).cpu().numpy(), port.spmv(s.r, s.c, s.v, x)) < 1e-12
     assert rel(A.apply(cuda(x), bs=s.bs).cpu().numpy(), port.spmv(s.r, s.c, s.v, x, s.bs)) < 1e-12
@@ -87,6 +108,44 @@ def test_padded_copy_products(d):
     y32 = A.apply_f32(cuda(x.astype(np.float32))).cpu().numpy()
     assert rel(y32, port.spmv(r, cols, v.astype(np.float32).astype(np.float64),
                               x.astype(np.float32).astype(np.float64))) < 1e-6
+    A.set_blocks(0)
+    assert A.padded == 0
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_padded_3x3_copy_with_overflow(d, precision):
+    """The slot-padded 3x3 copy: a rectangular matrix whose cells mostly carry
+    3-4 blocks (1 % none) while 1 % carry 9-12, so 4 slots hold every cell but those, which
+    keep 3 blocks in slots and the rest in the overflow list.  Full and row-0
+    float64 products and the float32 product against the oracle."""
+    from oracle import port
+    rng = np.random.default_rng(31)
+    ncell, mcell = 3000, 2000
+    pick = rng.choice(ncell, ncell // 50, replace=False).tolist()
+    wide, empty = set(pick[: ncell // 100]), set(pick[ncell // 100:])
+    rows, cols = [], []
+    for s_ in range(ncell):
+        nb = int(rng.integers(9, 13)) if s_ in wide else (0 if s_ in empty else int(rng.integers(3, 5)))
+        cs = np.sort(rng.choice(mcell, nb, replace=False))
+        for i in range(3):
+            for c_ in cs:
+                rows += [3 * s_ + i] * 3
+                cols += [3 * c_, 3 * c_ + 1, 3 * c_ + 2]
+    rows, cols = np.array(rows), np.array(cols, dtype=np.int32)
+    r = np.zeros(3 * ncell + 1, np.int32)
+    np.cumsum(np.bincount(rows, minlength=3 * ncell), out=r[1:])
+    v = rng.standard_normal(len(cols))
+    A = d.CSR(3 * ncell, 3 * mcell, r, cols, v)
+    A.set_blocks(3)
+    assert A.blocks[0] == 3 and A.padded == 4
+    x = rng.standard_normal(3 * mcell)
+    if precision == 64:
+        assert rel(A.apply(cuda(x)).cpu().numpy(), port.spmv(r, cols, v, x)) < 1e-12
+        assert rel(A.apply(cuda(x), bs=3).cpu().numpy(), port.spmv(r, cols, v, x, 3)) < 1e-12
+    else:
+        y32 = A.apply_f32(cuda(x.astype(np.float32))).cpu().numpy()
+        assert rel(y32, port.spmv(r, cols, v.astype(np.float32).astype(np.float64),
+                                  x.astype(np.float32).astype(np.float64))) < 1e-6
     A.set_blocks(0)
     assert A.padded == 0
 
