@@ -104,15 +104,17 @@ int deco_csr_set_blocks(deco_ctx ctx, deco_csr A, int bs);
 int deco_csr_blocks(deco_csr A, int* bs, int* nblk);
 /* Slots per cell of the padded copy that products of a 2x2-block matrix use
  * when every cell has at most 4 blocks (4 slots) or at most 7 or 8 blocks with
- * at most 25 % padding (7 or 8 slots), or slots per row of the scalar padded
- * copy that an FSAI factor without cell blocks gets (4, or 8 with at most 25 %
- * padding); 0 without one.  The block form is
+ * at most 25 % padding (7 or 8 slots); of a 3x3-block matrix, the fewest of 4, 7
+ * or 8 slots that leave at most 2 % of the cells wider (their further blocks
+ * go to an overflow list) within 25 % padding; or slots per row of the scalar
+ * padded copy that an FSAI factor without cell blocks gets (4, or 8 with at
+ * most 25 % padding); 0 without one.  The block forms are
  * made with the block copy; DECO_PADDED=0 in the environment at context
- * creation turns both off.  No counterpart in the reference. */
+ * creation turns them off.  No counterpart in the reference. */
 int deco_csr_padded(deco_csr A, int* slots);
 /* The product a full y = A x of this matrix takes for float64 (precision 64) or
  * float32 (32) values: kind 1 = the slot-padded copy (one thread per cell of
- * 2x2 blocks, or per scalar row: rows grouped per thread), 2 = the cell-block
+ * 2x2 or 3x3 blocks, or per scalar row: rows grouped per thread), 2 = the cell-block
  * kernel with `lanes` lanes per cell, 3 = the CSR kernel with `lanes` lanes per
  * row.  A CPR setup times the products each of its matrices has a layout for
  * and keeps the fastest (the layout rules' choice unless another is at least
@@ -153,9 +155,9 @@ int deco_fsai_info(deco_fsai F, int* n, int* nz, int* max_order);
 /* Cell-block copies of the two factors (deco_csr_set_blocks): block size (0
  * without) and stored blocks of FL and of FU^T. */
 int deco_fsai_blocks(deco_fsai F, int* bs, int* nblk_lower, int* nblk_upper);
-/* Padded slots of FL and FU^T (deco_csr_padded): per cell of their 2x2-block
- * copies, or per row for factors without cell blocks (the pressure FSAI); 4 for
- * power-1 factors of 7-point systems, 0 without.  No counterpart in the
+/* Padded slots of FL and FU^T (deco_csr_padded): per cell of their 2x2- or
+ * 3x3-block copies, or per row for factors without cell blocks (the pressure
+ * FSAI); 4 for power-1 factors of 7-point systems, 0 without.  No counterpart in the
  * reference. */
 int deco_fsai_padded(deco_fsai F, int* slots_lower, int* slots_upper);
 /* Bytes per slot column of FL's and FU^T's padded copies (deco_csr_slot_codes).
