@@ -219,7 +219,14 @@ def run_reference(args, rank, world):
     }))
 
 
-BATCH_WORKLOAD = "64 two-phase systems, cells log-uniform 10k-500k, 8 uniform right-hand sides each; CPR seq 3 + GMRES(50)"
+# the batched workload: 64 systems of 10k-500k cells (--batch-systems / --batch-cells
+# shrink it for profiler captures)
+BATCH_NSYS, BATCH_LO, BATCH_HI = 64, 10_000, 500_000
+
+
+def batch_workload():
+    return (f"{BATCH_NSYS} two-phase systems, cells log-uniform {BATCH_LO // 1000}k-{BATCH_HI // 1000}k, "
+            "8 uniform right-hand sides each; CPR seq 3 + GMRES(50)")
 
 
 def batch_result(steps, warmup, ctx, rank, world):
@@ -232,10 +239,10 @@ def batch_result(steps, warmup, ctx, rank, world):
     import deco_b200 as d
     from deco_b200 import gen, replicas
     st = ctx.torch_stream
-    r, c, v, ro, B, shapes = gen.batch(64, SEED, 10_000, 500_000, 2, 8)
+    r, c, v, ro, B, shapes = gen.batch(BATCH_NSYS, SEED, BATCH_LO, BATCH_HI, 2, 8)
     n_all, nnz_all = int(ro[-1]), len(c)
     if world > 1:
-        r, c, v, ro, B = gen.batch_subset(r, c, v, ro, B, 8, replicas.deal(64, rank, world))
+        r, c, v, ro, B = gen.batch_subset(r, c, v, ro, B, 8, replicas.deal(BATCH_NSYS, rank, world))
     n = int(ro[-1])
     dev = lambda a: torch.from_numpy(a).cuda()
     r_d, c_d, v_d, B_d = dev(r), dev(c), dev(v), dev(B)
@@ -278,7 +285,7 @@ def batch_result(steps, warmup, ctx, rank, world):
     out["mixed"]["max_err_vs_fp64"] = replicas.max_over_ranks(worst, device="cuda")
     del xs, X32, X64, r_d, c_d, v_d, B_d
     return {"value_s": out["mixed"]["time_s"], "steps": steps, "warmup": warmup,
-            "workload": f"{BATCH_WORKLOAD} ({n_all // 2} cells, {n_all} rows, {nnz_all} nnz)",
+            "workload": f"{batch_workload()} ({n_all // 2} cells, {n_all} rows, {nnz_all} nnz)",
             "parallelism": f"systems dealt round-robin to {world} GPU(s), no collective", **out,
             "speedup_mixed_vs_fp64": out["fp64"]["time_s"] / out["mixed"]["time_s"]}
 
@@ -297,7 +304,7 @@ def bench_batch(args):
     ctx = d.Context(int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_stream(ctx.torch_stream)
     b = batch_result(args.steps, args.warmup, ctx, rank, world)
-    line = {"metric": "batched CPR-GMRES time-to-1e-8 (64 systems x 8 right-hand sides)",
+    line = {"metric": f"batched CPR-GMRES time-to-1e-8 ({BATCH_NSYS} systems x 8 right-hand sides)",
             "value": b["value_s"], "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": False, "scaling": "strong", "dtype": "f32+f64",
             "data": "synthetic", "config": {"workload": b["workload"], "seed": SEED, "parallelism": b["parallelism"]},
@@ -524,6 +531,8 @@ def main():
                     help="timed steps of the config2 / adjoint / batch objects (one warm-up each)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only the per-kernel timings (for profiler captures on a smaller --config)")
+    ap.add_argument("--batch-systems", type=int, default=64, help="systems of the batched workload")
+    ap.add_argument("--batch-cells", default="10000,500000", help="LO,HI: cell counts of the batched systems")
     ap.add_argument("--config", type=int, default=3, help="system preset (3 = the 200x200x100 benchmark workload)")
     ap.add_argument("--grid", default=None,
                     help="NX,NY,NZ: the preset's distributions on a smaller grid (profiler captures)")
@@ -532,7 +541,9 @@ def main():
                          "adjoint: the 64x64x32 log-permeability gradient; "
                          "spmv: the SpMV kernels alone")
     args = ap.parse_args()
-    global CONFIG, GRID
+    global CONFIG, GRID, BATCH_NSYS, BATCH_LO, BATCH_HI
+    BATCH_NSYS = args.batch_systems
+    BATCH_LO, BATCH_HI = (int(t) for t in args.batch_cells.split(","))
     CONFIG = args.config
     GRID = tuple(int(t) for t in args.grid.split(",")) if args.grid else None
     if args.workload == "batch":

@@ -37,6 +37,11 @@ namespace {
 
 constexpr int kT = 256;            // threads per block of the batch kernels
 constexpr int kChunkRows = 4096;   // rows per dot chunk (chunks never cross systems)
+// blocks of the update pass per chunk (one per chunk left the 512-instance batch
+// with five and a fraction waves of long blocks, and small batches with a part of
+// the GPU; measured on 8 systems of 30k-100k cells: 211 blocks, 35 % of the DRAM
+// peak)
+constexpr int kUpdSub = 4;
 constexpr double kEpsB = 2.220446049250312e-16;
 // largest restart length: the kernels keep one coefficient per (basis column,
 // right-hand side) in dynamic shared memory, K (m + 1) doubles (32 KB at m = 512
@@ -348,9 +353,13 @@ __global__ void __launch_bounds__(kT) b_update_v(const int* crow, const int* csy
   extern __shared__ double cf_u[];  // [nc][K] coefficients
   __shared__ double part[(kT / 32) * P * E];
   __shared__ double tot[P * E];
-  const int c = blockIdx.x, sys = csys[c], nc = j + 1;
+  // blockIdx.y = sub-block: kUpdSub blocks share a chunk (interleaved vectors), so
+  // the grid has enough blocks to even out across the SMs; each writes its own
+  // partials, the finishing kernel sums them in a fixed order
+  const int c = blockIdx.x, sub = blockIdx.y, sys = csys[c], nc = j + 1;
+  double* __restrict__ redp = red + (long long)sub * K * nchunk;
   if (!in.sys_active[sys]) {
-    if (threadIdx.x < K) red[(long long)threadIdx.x * nchunk + c] = 0.0;
+    if (threadIdx.x < K) redp[(long long)threadIdx.x * nchunk + c] = 0.0;
     return;
   }
   for (int t = threadIdx.x; t < K * nc; t += kT) {
@@ -359,7 +368,8 @@ __global__ void __launch_bounds__(kT) b_update_v(const int* crow, const int* csy
   }
   __syncthreads();
   const long long f0 = (long long)crow[c] * K / E, f1 = (long long)crow[c + 1] * K / E;
-  const int ph = (int)((f0 + threadIdx.x) % P);
+  const long long fs = f0 + (long long)sub * kT;  // this sub-block's first vector
+  const int ph = (int)((fs + threadIdx.x) % P);
   double ss[E];
 #pragma unroll
   for (int q = 0; q < E; ++q) ss[q] = 0.0;
@@ -367,7 +377,7 @@ __global__ void __launch_bounds__(kT) b_update_v(const int* crow, const int* csy
   // products (UB independent loads per thread in flight; each element still
   // subtracts the columns in order)
   constexpr int UB = sizeof(T) == 4 ? 16 : 8;
-  for (long long f = f0 + threadIdx.x; f < f1; f += kT) {
+  for (long long f = fs + threadIdx.x; f < f1; f += (long long)kUpdSub * kT) {
     double x[E];
     vload<T, E>(w + f * E, x, false);
     int i = 0;
@@ -394,8 +404,8 @@ __global__ void __launch_bounds__(kT) b_update_v(const int* crow, const int* csy
     }
     vstore<T, E>(out + f * E, o);
   }
-  reduce_phase<P, E>(ss, part, (int)(f0 % P), tot);
-  for (int t2 = threadIdx.x; t2 < P * E; t2 += kT) red[(long long)t2 * nchunk + c] = tot[t2];
+  reduce_phase<P, E>(ss, part, (int)(fs % P), tot);
+  for (int t2 = threadIdx.x; t2 < P * E; t2 += kT) redp[(long long)t2 * nchunk + c] = tot[t2];
 }
 
 // one warp per instance: h, the Gram row of u_j, c = h + (h - G h), H(:,j), coefficients
@@ -451,7 +461,9 @@ __global__ void b_update_fin(int Q, const int* sch, BState st, Inst in, int j, c
   if (qi >= Q || !in.active[qi]) return;
   const int sys = qi / K, k = qi % K;
   double ss = 0.0;
-  for (int c = sch[sys]; c < sch[sys + 1]; ++c) ss += red[(long long)k * nchunk + c];
+  for (int c = sch[sys]; c < sch[sys + 1]; ++c)
+#pragma unroll
+    for (int sub = 0; sub < kUpdSub; ++sub) ss += red[((long long)sub * K + k) * nchunk + c];
   const double beta = sqrt(ss);
   st.H(qi, j + 1, j) = beta;
   st.s(qi)[j + 1] = beta != 0.0 ? 1.0 / beta : 0.0;
@@ -782,8 +794,8 @@ struct BatchSolver {
       b_dots_fin<K><<<(int)cdiv(Q, kT / 32), kT, sizeof(double) * (kT / 32) * (j + 1), s>>>(Q, sch, st, in, j,
                                                                                             red.get(), nch);
       DECO_CHECK_LAUNCH();
-      b_update_v<K, T><<<nch, kT, sizeof(double) * K * (j + 1), s>>>(crow, csys, st, in, ld, j, V.get(), w.get(),
-                                                                      col(j + 1), red.get(), nch);
+      b_update_v<K, T><<<dim3(nch, kUpdSub), kT, sizeof(double) * K * (j + 1), s>>>(crow, csys, st, in, ld, j, V.get(),
+                                                                                     w.get(), col(j + 1), red.get(), nch);
       DECO_CHECK_LAUNCH();
       b_update_fin<K><<<qb, 128, 0, s>>>(Q, sch, st, in, j, red.get(), nch, prm.reltol, prm.itmax);
       DECO_CHECK_LAUNCH();
