@@ -229,7 +229,7 @@ def batch_workload():
             "8 uniform right-hand sides each; CPR seq 3 + GMRES(50)")
 
 
-def batch_result(steps, warmup, ctx, rank, world):
+def batch_result(steps, warmup, ctx, rank, world, precisions=(32, 64)):
     """64 independent two-phase systems (cells log-uniform in 10k-500k), 8
     right-hand sides each, one lockstep CPR-GMRES solve per precision.  Under
     torchrun the systems are dealt round-robin to the ranks (replicas.deal:
@@ -248,7 +248,7 @@ def batch_result(steps, warmup, ctx, rank, world):
     r_d, c_d, v_d, B_d = dev(r), dev(c), dev(v), dev(B)
     out = {}
     xs = {}
-    for bits in (32, 64):
+    for bits in precisions:
         rows = []
         for k in range(warmup + steps):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -273,6 +273,12 @@ def batch_result(steps, warmup, ctx, rank, world):
             "iterations_median_rank0": float(statistics.median(it.ravel().tolist())),
             "max_true_rel_residual": replicas.max_over_ranks(float(rr.max()), device="cuda"),
             "widths": sorted(set(int(x) for x in w)), "instances_per_s": inst / (ms / 1e3)}
+    if 64 not in xs or 32 not in xs:  # one precision only (--no-fp64 on the batched line)
+        del xs, r_d, c_d, v_d, B_d
+        return {"value_s": out["mixed"]["time_s"], "steps": steps, "warmup": warmup,
+                "workload": f"{batch_workload()} ({n_all // 2} cells, {n_all} rows, {nnz_all} nnz)",
+                "parallelism": f"systems dealt round-robin to {world} GPU(s), no collective", **out,
+                "speedup_mixed_vs_fp64": None}
     # the mixed solutions' error against the float64 ones, per instance (columns of the multi-vector)
     X32, X64 = xs[32].view(-1, 8), xs[64].view(-1, 8)
     ro_t = torch.from_numpy(ro.astype("int64"))
@@ -303,12 +309,12 @@ def bench_batch(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     ctx = d.Context(int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_stream(ctx.torch_stream)
-    b = batch_result(args.steps, args.warmup, ctx, rank, world)
+    b = batch_result(args.steps, args.warmup, ctx, rank, world, (32,) if args.no_fp64 else (32, 64))
     line = {"metric": f"batched CPR-GMRES time-to-1e-8 ({BATCH_NSYS} systems x 8 right-hand sides)",
             "value": b["value_s"], "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": False, "scaling": "strong", "dtype": "f32+f64",
             "data": "synthetic", "config": {"workload": b["workload"], "seed": SEED, "parallelism": b["parallelism"]},
-            **{k: b[k] for k in ("mixed", "fp64", "speedup_mixed_vs_fp64")}}
+            **{k: b[k] for k in ("mixed", "fp64", "speedup_mixed_vs_fp64") if k in b}}
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

@@ -604,20 +604,26 @@ __device__ __forceinline__ void group_row(int q, int nq, const int* __restrict__
   solve_row_group<S>(q < nq ? rows[q] : -1, gP + g0, gB + g0, gPv + g0, Ar, Ac, Av, Fr, Fc, FLv, FUv);
 }
 
+// KR: the register order of class 1 (4 when no row is wider, 8 otherwise);
+// WIDE: whether classes 2-4 occur.  The narrow instantiations carry only the
+// class-1 code, so they need far fewer registers (more rows in flight per SM);
+// the launch still covers every row of the factor.
+template <int KR, bool WIDE>
 __global__ void __launch_bounds__(kLuBlock) fsai_local_systems(
     const int* __restrict__ perm, int4 cnt, int4 off, int b1, int b2, int b3, const int* __restrict__ Ar,
     const int* __restrict__ Ac, const double* __restrict__ Av, const int* __restrict__ Fr,
     const int* __restrict__ Fc, double* __restrict__ FLv, double* __restrict__ FUv) {
   extern __shared__ double smem[];
-  __shared__ int gP[kLuBlock];
-  __shared__ double gB[kLuBlock];
-  __shared__ int gPv[kLuBlock];
+  __shared__ int gP[WIDE ? kLuBlock : 1];
+  __shared__ double gB[WIDE ? kLuBlock : 1];
+  __shared__ int gPv[WIDE ? kLuBlock : 1];
   const int b = blockIdx.x;
   if (b < b1) {
     const int q = b * kLuBlock + threadIdx.x;
-    if (q < cnt.x) solve_row_reg<8>(perm[off.x + q], Ar, Ac, Av, Fr, Fc, FLv, FUv);
+    if (q < cnt.x) solve_row_reg<KR>(perm[off.x + q], Ar, Ac, Av, Fr, Fc, FLv, FUv);
     return;
   }
+  if constexpr (WIDE) {
   if (b < b2) {
     group_row<16>((b - b1) * (kLuBlock / 16) + threadIdx.x / 16, cnt.y, perm + off.y, gP, gB, gPv, Ar, Ac, Av, Fr,
                   Fc, FLv, FUv);
@@ -633,6 +639,7 @@ __global__ void __launch_bounds__(kLuBlock) fsai_local_systems(
   double* base = smem;  // 64x64 system (32 KB), then rhs and pivots
   double* rl = smem + 64 * 64;
   solve_row_warp(perm[off.w + q], base, rl, rl + 64, reinterpret_cast<int*>(rl + 128), Ar, Ac, Av, Fr, Fc, FLv, FUv);
+  }
 }
 
 // ------------------------------------------------- D-scaling (diagonal.cpp)
@@ -850,11 +857,22 @@ void fsai_build(deco_ctx_s* ctx, const deco_csr_s* A0, double tol_rel, double to
     const int b3 = b2 + (int)cdiv(n3, kLuBlock / 32);
     const int nblk = b3 + n4;
     const size_t smem = n4 > 0 ? kSmemBytes : 0;
-    if (smem) DECO_CUDA(cudaFuncSetAttribute(fsai_local_systems, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
-    fsai_local_systems<<<nblk, kLuBlock, smem, st>>>(perm.get(), make_int4(n1, n2, n3, n4),
-                                                      make_int4(0, n1, n1 + n2, n1 + n2 + n3), b1, b2, b3,
-                                                      A->r.get(), A->c.get(), A->v.get(), FL.r.get(), FL.c.get(),
-                                                      FL.v.get(), fu.get());
+    const int4 cnt4 = make_int4(n1, n2, n3, n4), off4 = make_int4(0, n1, n1 + n2, n1 + n2 + n3);
+    if (n2 + n3 + n4 > 0) {
+      if (smem) DECO_CUDA(cudaFuncSetAttribute(fsai_local_systems<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               kSmemBytes));
+      fsai_local_systems<8, true><<<nblk, kLuBlock, smem, st>>>(perm.get(), cnt4, off4, b1, b2, b3, A->r.get(),
+                                                                A->c.get(), A->v.get(), FL.r.get(), FL.c.get(),
+                                                                FL.v.get(), fu.get());
+    } else if (h[8] <= 4) {
+      fsai_local_systems<4, false><<<nblk, kLuBlock, 0, st>>>(perm.get(), cnt4, off4, b1, b2, b3, A->r.get(),
+                                                              A->c.get(), A->v.get(), FL.r.get(), FL.c.get(),
+                                                              FL.v.get(), fu.get());
+    } else {
+      fsai_local_systems<8, false><<<nblk, kLuBlock, 0, st>>>(perm.get(), cnt4, off4, b1, b2, b3, A->r.get(),
+                                                              A->c.get(), A->v.get(), FL.r.get(), FL.c.get(),
+                                                              FL.v.get(), fu.get());
+    }
     DECO_CHECK_LAUNCH();
   }
   trace_mark(ctx, "fsai local systems");
