@@ -124,6 +124,37 @@ __device__ void finalize_partials(const double* red, int nb, int ncols, double* 
   }
 }
 
+// The same reduction for nb <= 32 MAXB partials per column, with every load of
+// four columns issued before the sums (up to 4 MAXB loads in flight per lane
+// instead of 16); each column sums in the same lane-strided order, so the result
+// is identical.  For the last block of the dot pass, which holds up the next
+// kernel while it runs.
+template <int MAXB>
+__device__ void finalize_partials_wide(const double* red, int nb, int ncols, double* out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int i0 = warp; i0 < ncols; i0 += 4 * kWarps) {
+    double v[4][MAXB];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const double* p = red + (size_t)min(i0 + u * kWarps, ncols - 1) * nb;
+#pragma unroll
+      for (int t = 0; t < MAXB; ++t) {
+        const int b = lane + 32 * t;
+        v[u][t] = b < nb ? __ldcg(p + b) : 0.0;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      double s = 0.0;
+#pragma unroll
+      for (int t = 0; t < MAXB; ++t)
+        if (lane + 32 * t < nb) s += v[u][t];
+      const double tot = warp_sum(s);
+      if (lane == 0 && i0 + u * kWarps < ncols) out[i0 + u * kWarps] = tot;
+    }
+  }
+}
+
 // true in the block that finishes last (no waiting: an atomic ticket)
 __device__ __forceinline__ bool last_block(unsigned* counter) {
   __shared__ bool amlast;
@@ -181,7 +212,8 @@ template <> struct Vec4<double> {
 // last block of pass A: h, the new Gram row, c = h + (h - G h) and H(:,j);
 // hs: ncols doubles of shared memory
 __device__ void dots_finish(int ncols, int j, const double* __restrict__ red, State st, double* hs) {
-  finalize_partials(red, gridDim.x, 2 * ncols, st.sums);
+  if (gridDim.x <= 32 * 10) finalize_partials_wide<10>(red, gridDim.x, 2 * ncols, st.sums);
+  else finalize_partials(red, gridDim.x, 2 * ncols, st.sums);
   __syncthreads();
   // h_i = s_i (u_i . w);  G(i,j) = s_i s_j (u_i . u_j)
   const double sj = st.s[j];
@@ -197,7 +229,7 @@ __device__ void dots_finish(int ncols, int j, const double* __restrict__ red, St
   // are in flight while the sum runs in order)
   for (int i = threadIdx.x; i < ncols; i += kThreads) {
     double gh = 0.0;
-#pragma unroll 8
+#pragma unroll 32
     for (int k = 0; k < ncols; ++k) gh += st.gm(i, k) * hs[k];
     const double ci = hs[i] + (hs[i] - gh);
     st.h(i, j) = ci;
