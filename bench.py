@@ -770,6 +770,12 @@ def main():
             "what": "arnoldi_dots + arnoldi_update per Arnoldi step, float32 basis, mean over the solve's steps "
                     f"(restart {m}, {it} iterations)",
             "phase_ms_per_iteration": {k: v / max(1, it) for k, v in info["phases_ms"].items()}}
+        # each pass alone: (j + 3) 4n bytes per step (the j + 1 columns, w, and u_j read or u_{j+1} written)
+        t_d = info["phases_ms"]["dots"] / max(1, it)
+        for name, t, what in (("arnoldi_dots_f32", t_d, "dot pass (arnoldi_dots / arnoldi_dots_bulk)"),
+                              ("arnoldi_update_f32", t_o - t_d, "update pass (arnoldi_update)")):
+            kernels[name] = {"ms": t, "gbs": (alg_o / 2) / t / 1e6, "alg_bytes": alg_o / 2,
+                             "what": f"{what} per Arnoldi step, float32 basis, mean over the solve's steps"}
     for k in kernels.values():
         k["frac_of_peak"] = k["gbs"] / peak
     dom = kernels["spmv_A_f32"]

@@ -480,7 +480,8 @@ class SOL:
         self.res_abs, self.res_rel = res.res_abs, res.res_rel
         self.res_rel_orig = res.res_rel_orig
         self.time_ms, self.restarts = res.t_solve_ms, res.restarts
-        self.phases_ms = {"precond": res.t_precond_ms, "matvec": res.t_matvec_ms, "ortho": res.t_ortho_ms}
+        self.phases_ms = {"precond": res.t_precond_ms, "matvec": res.t_matvec_ms, "ortho": res.t_ortho_ms,
+                          "dots": res.t_dots_ms}
         self.resvec = self.resvec[: self.iter]
 
     def get_result(self):

@@ -34,7 +34,8 @@ class SolParams(C.Structure):
 class SolResult(C.Structure):
     _fields_ = [("iter", C.c_int), ("flag", C.c_int), ("res_abs", C.c_double), ("res_rel", C.c_double),
                 ("t_solve_ms", C.c_double), ("restarts", C.c_int), ("t_precond_ms", C.c_double),
-                ("t_matvec_ms", C.c_double), ("t_ortho_ms", C.c_double), ("res_rel_orig", C.c_double)]
+                ("t_matvec_ms", C.c_double), ("t_ortho_ms", C.c_double), ("res_rel_orig", C.c_double),
+                ("t_dots_ms", C.c_double)]
 
 
 class BatchResult(C.Structure):

@@ -27,9 +27,10 @@ __global__ void to_f32(const double* __restrict__ a, float* __restrict__ b, long
 }
 
 // one thread per cell: the number of distinct block columns over its bs rows
-// (each row's columns are ascending, so its block columns are too)
-__global__ void bsr_count(int nbr, int bs, const int* __restrict__ r, const int* __restrict__ c,
-                          int* __restrict__ cnt) {
+// (each row's columns are ascending, so its block columns are too); bs is a
+// template argument so the divisions by it compile to multiplications
+template <int bs>
+__global__ void bsr_count(int nbr, const int* __restrict__ r, const int* __restrict__ c, int* __restrict__ cnt) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nbr; s += gridDim.x * blockDim.x) {
     int pos[3], end[3];
     for (int q = 0; q < bs; ++q) { pos[q] = r[s * bs + q]; end[q] = r[s * bs + q + 1]; }
@@ -49,9 +50,9 @@ __global__ void bsr_count(int nbr, int bs, const int* __restrict__ r, const int*
 
 // the same merge, writing block columns and the values into their row planes
 // (bv is zero-filled beforehand: absent entries stay zero)
-__global__ void bsr_fill(int nbr, int bs, const int* __restrict__ r, const int* __restrict__ c,
-                         const double* __restrict__ v, const int* __restrict__ br, int* __restrict__ bc,
-                         double* __restrict__ bv, long long plane) {
+template <int bs>
+__global__ void bsr_fill(int nbr, const int* __restrict__ r, const int* __restrict__ c, const double* __restrict__ v,
+                         const int* __restrict__ br, int* __restrict__ bc, double* __restrict__ bv, long long plane) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nbr; s += gridDim.x * blockDim.x) {
     int pos[3], end[3];
     for (int q = 0; q < bs; ++q) { pos[q] = r[s * bs + q]; end[q] = r[s * bs + q + 1]; }
@@ -401,7 +402,8 @@ void make_bsr(deco_ctx_s* ctx, deco_csr_s* A, int bs, double max_fill) {
   const int nbr = A->n / bs;
   DevBuf<int> cnt(nbr + 1, st);
   const int g = grid_for(ctx, nbr, 256);
-  bsr_count<<<g, 256, 0, st>>>(nbr, bs, A->r.get(), A->c.get(), cnt.get());
+  if (bs == 2) bsr_count<2><<<g, 256, 0, st>>>(nbr, A->r.get(), A->c.get(), cnt.get());
+  else bsr_count<3><<<g, 256, 0, st>>>(nbr, A->r.get(), A->c.get(), cnt.get());
   DECO_CHECK_LAUNCH();
   DevBuf<int> br(nbr + 1, st);
   const long long nblk = exclusive_scan_int(ctx, cnt.get(), br.get(), nbr);
@@ -413,8 +415,12 @@ void make_bsr(deco_ctx_s* ctx, deco_csr_s* A, int bs, double max_fill) {
   A->bplane = plane;
   A->bv.alloc(plane * bs, st);
   A->bv.zero(st);
-  bsr_fill<<<g, 256, 0, st>>>(nbr, bs, A->r.get(), A->c.get(), A->v.get(), A->br.get(), A->bc.get(), A->bv.get(),
-                              plane);
+  if (bs == 2)
+    bsr_fill<2><<<g, 256, 0, st>>>(nbr, A->r.get(), A->c.get(), A->v.get(), A->br.get(), A->bc.get(), A->bv.get(),
+                                   plane);
+  else
+    bsr_fill<3><<<g, 256, 0, st>>>(nbr, A->r.get(), A->c.get(), A->v.get(), A->br.get(), A->bc.get(), A->bv.get(),
+                                   plane);
   DECO_CHECK_LAUNCH();
   A->bbs = bs;
   A->avg_blk = double(nblk) / nbr;

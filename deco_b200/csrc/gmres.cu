@@ -991,7 +991,7 @@ struct Solver {
   bool profile = false;
   int lookahead = 3;  // Arnoldi steps queued beyond the one whose |g| the host is waiting for
   std::vector<cudaEvent_t> pev;
-  double t_phase[3] = {0, 0, 0};
+  double t_phase[4] = {0, 0, 0, 0};  // precond, matvec, dot pass, update pass
   // the |g| ring: host views, device views, and the tag each slot waits for
   volatile double* hval = nullptr;
   volatile unsigned long long* htag = nullptr;
@@ -1022,7 +1022,7 @@ struct Solver {
     if (const char* e = std::getenv("DECO_PROFILE")) profile = std::atoi(e) != 0;
     if (const char* e = std::getenv("DECO_LOOKAHEAD")) lookahead = std::max(0, std::min(kRing - 2, std::atoi(e)));
     if (profile) {
-      pev.resize(4 * (size_t)(m + 1));
+      pev.resize(5 * (size_t)(m + 1));
       for (auto& e : pev) DECO_CUDA(cudaEventCreate(&e));
     }
     trace_mark(ctx, "gmres: allocate");
@@ -1032,13 +1032,9 @@ struct Solver {
   void collect(int steps) {
     if (!profile) return;
     for (int j = 0; j < steps; ++j) {
-      float a = 0, b = 0, c = 0;
-      DECO_CUDA(cudaEventElapsedTime(&a, pev[4 * j], pev[4 * j + 1]));
-      DECO_CUDA(cudaEventElapsedTime(&b, pev[4 * j + 1], pev[4 * j + 2]));
-      DECO_CUDA(cudaEventElapsedTime(&c, pev[4 * j + 2], pev[4 * j + 3]));
-      t_phase[0] += a;
-      t_phase[1] += b;
-      t_phase[2] += c;
+      float t[4] = {0, 0, 0, 0};
+      for (int q = 0; q < 4; ++q) DECO_CUDA(cudaEventElapsedTime(&t[q], pev[5 * j + q], pev[5 * j + q + 1]));
+      for (int q = 0; q < 4; ++q) t_phase[q] += t[q];
     }
   }
 
@@ -1084,22 +1080,23 @@ struct Solver {
   void arnoldi_step(int j, bool left) {
     cudaStream_t s = ctx->stream;
     const double* sj = st.s + j;
-    // phase order per step: [pev0] precond [pev1] matvec [pev2] ortho [pev3]
-    // (left GMRES runs the matvec first; its phases are recorded accordingly)
-    if (profile) DECO_CUDA(cudaEventRecord(pev[4 * j], s));
+    // phase order per step: [pev0] precond [pev1] matvec [pev2] dot pass [pev3] update
+    // pass [pev4] (left GMRES runs the matvec first; its phases are recorded accordingly)
+    if (profile) DECO_CUDA(cudaEventRecord(pev[5 * j], s));
     if (!left) {
       precond<T, T>(col(j), z.get());
-      if (profile) DECO_CUDA(cudaEventRecord(pev[4 * j + 1], s));
+      if (profile) DECO_CUDA(cudaEventRecord(pev[5 * j + 1], s));
       matvec_scaled<T>(z.get(), w.get(), sj);
     } else {
       matvec_scaled<T>(col(j), z.get(), sj);
-      if (profile) DECO_CUDA(cudaEventRecord(pev[4 * j + 1], s));
+      if (profile) DECO_CUDA(cudaEventRecord(pev[5 * j + 1], s));
       precond<T, T>(z.get(), w.get());
     }
-    if (profile) DECO_CUDA(cudaEventRecord(pev[4 * j + 2], s));
+    if (profile) DECO_CUDA(cudaEventRecord(pev[5 * j + 2], s));
     const int nc = j + 1;
     launch_arnoldi_dots<T>(s, nb, n, ld, nc, j, V.get(), w.get(), ctx->red.get(), ctx->counter.get(), st);
     DECO_CHECK_LAUNCH();
+    if (profile) DECO_CUDA(cudaEventRecord(pev[5 * j + 3], s));
     HostSlot hs;
     hs.val = dval + j % kRing;
     hs.tag = dtag + j % kRing;
@@ -1108,7 +1105,7 @@ struct Solver {
     launch_k(arnoldi_update<T>, nb, kThreads, smem_for_blocks(4, sizeof(double) * 4 * (nc + 1)), s, n, ld, nc, j,
              V.get(), w.get(), col(j + 1), ctx->red.get(), ctx->counter.get(), st, hs);
     DECO_CHECK_LAUNCH();
-    if (profile) DECO_CUDA(cudaEventRecord(pev[4 * j + 3], s));
+    if (profile) DECO_CUDA(cudaEventRecord(pev[5 * j + 4], s));
   }
 
   // |g_{j+1}| of step j, once the update pass has posted it.  The host polls
@@ -1231,7 +1228,8 @@ struct Solver {
     res->restarts = restarts;
     res->t_precond_ms = t_phase[0];
     res->t_matvec_ms = t_phase[1];
-    res->t_ortho_ms = t_phase[2];
+    res->t_ortho_ms = t_phase[2] + t_phase[3];
+    res->t_dots_ms = t_phase[2];
     // the residual of the original (not decoupled) system: b - A x on the
     // decoupled system, mapped back through the inverse of the CPR's decoupling
     spmv<double, double>(ctx, A, x, EpiResid<double, double>{b, xtmp.get()});

@@ -268,6 +268,9 @@ typedef struct deco_sol_result {
    * decoupling rewrote A and b (res_rel is on the decoupled system, as the
    * reference reports it).  Equals the true relative residual when P is NULL. */
   double res_rel_orig;
+  /* with DECO_PROFILE=1: the part of t_ortho_ms spent in the dot pass (the rest
+   * is the update pass) */
+  double t_dots_ms;
 } deco_sol_result;
 
 /* Solves A x = b with preconditioner P (NULL: identity).  A and d_b are the
