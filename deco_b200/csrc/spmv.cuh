@@ -42,13 +42,13 @@ struct deco_csr_s {
   deco::DevBuf<float> bv32;
   int bsw64 = 0, bsw32 = 0;
   double avg_blk = 0;
-  // Slot-padded copy (bbs == 2: of the cell blocks; bbs == 0: of the scalar rows,
-  // ec[k * n + i] / ev[k * n + i] holding row i's entry k).
-  // Slot-padded copy of a 2x2-block matrix whose cells have at most `ew` blocks
-  // (ew = 4, 7 or 8 for cell blocks, 4 or 8 for scalar rows; 0: none): every cell gets ew block slots, slot-major (slot k of
-  // all cells contiguous), unused slots repeating one of the cell's columns (or
-  // column 0) with zero values.  ec[k * ncell + s]: block column; value plane q (in-block row q),
-  // slot k: the block row's two values at pair index (q * ew + k) * ncell + s.
+  // Slot-padded copy (bbs == 2 or 3: of the cell blocks; bbs == 0: of the scalar
+  // rows, ec[k * n + i] / ev[k * n + i] holding row i's entry k).  ew = 4, 7 or 8
+  // slots per cell (4 or 8 per scalar row; 0: none), slot-major (slot k of all
+  // cells contiguous), unused slots repeating one of the cell's columns (or
+  // column 0) with zero values.  2x2 cells (at most ew blocks each):
+  // ec[k * ncell + s] is the block column, value plane q (in-block row q), slot k
+  // the block row's two values at pair index (q * ew + k) * ncell + s.
   int ew = 0;
   deco::DevBuf<int> ec;
   deco::DevBuf<double> ev;
