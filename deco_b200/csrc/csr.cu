@@ -331,18 +331,37 @@ void make_padded(deco_ctx_s* ctx, deco_csr_s* A) {
   }
 }
 
-// slot-major padded scalar rows (columns too when ec != nullptr)
+// slot-major padded scalar rows (columns too when ec != nullptr); a row with more
+// than W entries (ostart != nullptr) keeps W - 1 in slots, marks the last slot
+// with column -1 and puts the rest in the overflow list from ostart[i]
 template <typename T>
 __global__ void ell1_fill(int n, int W, const int* __restrict__ r, const int* __restrict__ c, const T* __restrict__ v,
-                          int* __restrict__ ec, T* __restrict__ ev) {
+                          const int* __restrict__ ostart, int* __restrict__ ec, T* __restrict__ ev,
+                          int* __restrict__ oc, T* __restrict__ ov) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int a = r[i], e = r[i + 1];
+    const bool over = e - a > W;
     for (int k = 0; k < W; ++k) {
-      const bool on = a + k < e;
+      const bool mark = over && k == W - 1;
+      const bool on = !mark && a + k < e;
       // an unused slot reads a column the row already has (or column 0) with a zero value
-      if (ec) ec[(long long)k * n + i] = on ? c[a + k] : (e > a ? c[a] : 0);
+      if (ec) ec[(long long)k * n + i] = mark ? -1 : (on ? c[a + k] : (e > a ? c[a] : 0));
       ev[(long long)k * n + i] = on ? v[a + k] : (T)0;
     }
+    if (over)
+      for (int t = a + W - 1; t < e; ++t) {
+        const int o = ostart[i] + t - (a + W - 1);
+        if (oc) oc[o] = c[t];
+        ov[o] = v[t];
+      }
+  }
+}
+
+// entries of row i past its first W - 1 when it has more than W (0 otherwise)
+__global__ void row_overflow_count(const int* __restrict__ r, int n, int W, int* __restrict__ cnt) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int len = r[i + 1] - r[i];
+    cnt[i] = len > W ? len - (W - 1) : 0;
   }
 }
 
@@ -354,20 +373,44 @@ void make_padded_scalar(deco_ctx_s* ctx, deco_csr_s* A) {
     int W = 0;
     if (A->max_row <= 4) W = 4;
     else if (A->max_row <= 8 && 8.0 * n <= 1.25 * A->nz) W = 8;
+    else {  // 4 or 8 slots when at most 2 % of the rows are longer (their rest: the overflow list)
+      DevBuf<int> hist(kHistCap + 1, st);
+      hist.zero(st);
+      block_hist<<<grid_for(ctx, n, 256), 256, 0, st>>>(A->r.get(), n, hist.get());
+      DECO_CHECK_LAUNCH();
+      std::vector<int> h(kHistCap + 1);
+      DECO_CUDA(cudaMemcpyAsync(h.data(), hist.get(), sizeof(int) * h.size(), cudaMemcpyDeviceToHost, st));
+      DECO_CUDA(cudaStreamSynchronize(st));
+      for (int cand : {4, 8}) {
+        long long over = 0;
+        for (int b = cand + 1; b <= kHistCap; ++b) over += h[b];
+        if (over <= n / 50 && (double)cand * n <= 1.25 * A->nz && h[kHistCap] == 0) { W = cand; break; }
+      }
+    }
     if (!W) return;
     A->ew = W;
     A->ec.alloc((size_t)W * n, st);
     A->ev.alloc((size_t)W * n, st);
-    ell1_fill<double><<<grid_for(ctx, n, 256), 256, 0, st>>>(n, W, A->r.get(), A->c.get(), A->v.get(), A->ec.get(),
-                                                              A->ev.get());
+    if (A->max_row > W) {
+      DevBuf<int> cnt(n + 1, st), ostart(n + 1, st);
+      row_overflow_count<<<grid_for(ctx, n, 256), 256, 0, st>>>(A->r.get(), n, W, cnt.get());
+      DECO_CHECK_LAUNCH();
+      A->nov = (int)exclusive_scan_int(ctx, cnt.get(), ostart.get(), n);
+      A->eo = std::move(ostart);
+      A->oc.alloc(std::max(A->nov, 1), st);
+      A->ov.alloc(std::max(A->nov, 1), st);
+    }
+    ell1_fill<double><<<grid_for(ctx, n, 256), 256, 0, st>>>(n, W, A->r.get(), A->c.get(), A->v.get(), A->eo.get(),
+                                                              A->ec.get(), A->ev.get(), A->oc.get(), A->ov.get());
     DECO_CHECK_LAUNCH();
-    make_slot_codes(ctx, A, n);
+    if (!A->nov) make_slot_codes(ctx, A, n);  // a marked slot has no offset to code
   }
   if (A->v32) {
     const int W = A->ew;
     if (!A->ev32 || A->ev32.size() != (size_t)W * n) A->ev32.alloc((size_t)W * n, st);
-    ell1_fill<float><<<grid_for(ctx, n, 256), 256, 0, st>>>(n, W, A->r.get(), A->c.get(), A->v32.get(), nullptr,
-                                                             A->ev32.get());
+    if (A->nov && (!A->ov32 || A->ov32.size() != (size_t)A->nov)) A->ov32.alloc(A->nov, st);
+    ell1_fill<float><<<grid_for(ctx, n, 256), 256, 0, st>>>(n, W, A->r.get(), A->c.get(), A->v32.get(), A->eo.get(),
+                                                             nullptr, A->ev32.get(), nullptr, A->ov32.get());
     DECO_CHECK_LAUNCH();
   }
 }
@@ -450,6 +493,11 @@ void refresh_stats(deco_ctx_s* ctx, deco_csr_s* A) {
     A->eb = A->noff = 0;
     A->ecode = DevBuf<unsigned char>();
     A->eoff = DevBuf<int>();
+    A->nov = 0;
+    A->eo = DevBuf<int>();
+    A->oc = DevBuf<int>();
+    A->ov = DevBuf<double>();
+    A->ov32 = DevBuf<float>();
   }
 }
 

@@ -446,7 +446,7 @@ void spmm(deco_ctx_s* ctx, const deco_csr_s* A, const XT* x, Epi epi, bool row0 
     else gate = MMGate{};
   }
   cudaStream_t st = ctx->stream;
-  if (A->ew && (M.bs == 2 || (M.bs == 1 && !A->bbs && !row0))) {
+  if (A->ew && !A->nov && (M.bs == 2 || (M.bs == 1 && !A->bbs && !row0))) {  // (no overflow lists here)
     const VT* ev;
     if constexpr (sizeof(VT) == 4) ev = A->ev32.get(); else ev = A->ev.get();
     if (ev) {

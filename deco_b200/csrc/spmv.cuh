@@ -546,7 +546,10 @@ template <int W, typename VT, typename XT, class Epi, int EB = 0>
 __global__ void __launch_bounds__(256) ell1_kernel(int n, const int* __restrict__ ec, const VT* __restrict__ ev,
                                                    const XT* __restrict__ x, Epi epi,
                                                    const unsigned char* __restrict__ code = nullptr,
-                                                   const int* __restrict__ off = nullptr) {
+                                                   const int* __restrict__ off = nullptr,
+                                                   const int* __restrict__ eo = nullptr,
+                                                   const int* __restrict__ oc = nullptr,
+                                                   const VT* __restrict__ ov = nullptr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int cc[W];
@@ -558,6 +561,10 @@ __global__ void __launch_bounds__(256) ell1_kernel(int n, const int* __restrict_
   }
   pdl_wait();
   pdl_trigger();
+  // a row longer than the slots marks its last slot with column -1 (value 0) and
+  // keeps the rest of its entries in the overflow list, added after the slots
+  const bool over = EB == 0 && cc[W - 1] < 0;
+  if (over) cc[W - 1] = 0;
   double sum = 0.0;
   if constexpr (kRunF32<VT, XT>) {
 #pragma unroll
@@ -571,6 +578,13 @@ __global__ void __launch_bounds__(256) ell1_kernel(int n, const int* __restrict_
 #pragma unroll
     for (int k = 0; k < W; ++k) sum += (double)vv[k] * (double)__ldg(x + cc[k]);
   }
+  if (over) {
+    const int o0 = eo[i], o1 = eo[i + 1];
+    for (int o = o0; o < o1; ++o) {
+      if constexpr (kRunF32<VT, XT>) sum += (double)(ov[o] * __ldg(x + oc[o]));
+      else sum += (double)ov[o] * (double)__ldg(x + oc[o]);
+    }
+  }
   epi(i, sum);
 }
 
@@ -578,14 +592,19 @@ template <typename VT, typename XT, class Epi>
 void launch_ell1(cudaStream_t st, const deco_csr_s* A, const XT* x, Epi epi) {
   if (A->n <= 0) return;
   const VT* ev;
-  if constexpr (sizeof(VT) == 4) ev = A->ev32.get(); else ev = A->ev.get();
+  const VT* ov;
+  if constexpr (sizeof(VT) == 4) { ev = A->ev32.get(); ov = A->ov32.get(); } else { ev = A->ev.get(); ov = A->ov.get(); }
   const unsigned grid = (unsigned)cdiv(A->n, 256);
   const unsigned char* cd = A->ecode.get();
   const int* of = A->eoff.get();
   auto go = [&](auto eb) {
     constexpr int EB = decltype(eb)::value;
-    if (A->ew == 4) launch_k(ell1_kernel<4, VT, XT, Epi, EB>, grid, 256, 0, st, A->n, A->ec.get(), ev, x, epi, cd, of);
-    else launch_k(ell1_kernel<8, VT, XT, Epi, EB>, grid, 256, 0, st, A->n, A->ec.get(), ev, x, epi, cd, of);
+    if (A->ew == 4)
+      launch_k(ell1_kernel<4, VT, XT, Epi, EB>, grid, 256, 0, st, A->n, A->ec.get(), ev, x, epi, cd, of, A->eo.get(),
+               A->oc.get(), ov);
+    else
+      launch_k(ell1_kernel<8, VT, XT, Epi, EB>, grid, 256, 0, st, A->n, A->ec.get(), ev, x, epi, cd, of, A->eo.get(),
+               A->oc.get(), ov);
   };
   if (A->eb == 1) go(std::integral_constant<int, 1>{});
   else if (A->eb == 2) go(std::integral_constant<int, 2>{});

@@ -150,6 +150,32 @@ def test_padded_3x3_copy_with_overflow(d, precision):
     assert A.padded == 0
 
 
+@pytest.mark.parametrize("precision", [64, 32])
+def test_padded_copies_of_three_phase_cpr_with_faults(d, precision):
+    """A three-phase system with fault connections: its global FSAI factors get the
+    3x3 padded copy, and its pressure FSAI factors the scalar one with 4 slots, the
+    rows lengthened by a fault (1.4 % of them) finishing from the overflow list.
+    The CPR apply keeps the parity bar against the oracle and the solve its
+    iteration count (mixed precision: a solve that float64 finishes inside one
+    restart cycle takes one more refinement cycle, so there the bar is the count
+    plus one cycle)."""
+    from oracle import port
+    s = SYSTEMS["bs3_faults"]()
+    prec = cpr_json(3)
+    A = d.CSR.from_system(s)
+    b = cuda(s.b)
+    P = d.CPR(prec, A, b, precision)
+    assert P.fsai(0).padded[0] in (4, 7, 8) and P.fsai(1).padded == (4, 4)
+    O = port.Cpr(prec, s.r, s.c, s.v, s.b)
+    rvec = np.random.default_rng(6).standard_normal(s.n)
+    tol = 1e-12 if precision == 64 else 1e-5
+    assert rel(P.apply(cuda(rvec)).cpu().numpy(), O.apply(rvec)) < tol
+    S = d.SOL(sol_json(), A, P, b, precision=precision)
+    ref_it = O.solve(sol_json())["iter"]
+    slack = max(2, 0.1 * ref_it) if precision == 64 else int(sol_json()["restart"])
+    assert S.flag == 0 and abs(S.iter - ref_it) <= slack
+
+
 def test_padding_with_zeros(d):
     """Entries missing from a cell block (a filtered pattern) are stored as zeros."""
     from oracle import port
