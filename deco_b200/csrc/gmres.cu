@@ -990,6 +990,7 @@ struct Solver {
   // DECO_PROFILE=1: events around the phases of every Arnoldi step of a cycle
   bool profile = false;
   int lookahead = 3;  // Arnoldi steps queued beyond the one whose |g| the host is waiting for
+  double step_timeout_ms = 600e3;
   std::vector<cudaEvent_t> pev;
   double t_phase[4] = {0, 0, 0, 0};  // precond, matvec, dot pass, update pass
   // the |g| ring: host views, device views, and the tag each slot waits for
@@ -1021,6 +1022,7 @@ struct Solver {
     if (ctx->red.size() < need) ctx->red.alloc(need, s);
     if (const char* e = std::getenv("DECO_PROFILE")) profile = std::atoi(e) != 0;
     if (const char* e = std::getenv("DECO_LOOKAHEAD")) lookahead = std::max(0, std::min(kRing - 2, std::atoi(e)));
+    if (const char* e = std::getenv("DECO_STEP_TIMEOUT")) step_timeout_ms = std::max(1.0, std::atof(e)) * 1e3;
     if (profile) {
       pev.resize(5 * (size_t)(m + 1));
       for (auto& e : pev) DECO_CUDA(cudaEventCreate(&e));
@@ -1109,10 +1111,13 @@ struct Solver {
   }
 
   // |g_{j+1}| of step j, once the update pass has posted it.  The host polls
-  // the tag; every 1024 polls it asks the stream whether it failed or drained.
+  // the tag; every 1024 polls it asks the stream whether it failed or drained,
+  // and gives up (DECO_ERR_CUDA) when the step has not finished after
+  // DECO_STEP_TIMEOUT seconds (default 600).
   double step_result(int j) {
     const int slot = j % kRing;
     volatile unsigned long long* tp = htag + slot;
+    double t0 = -1.0;
     for (unsigned long long spin = 1; *tp != tags[slot]; ++spin) {
       if ((spin & 1023) == 0) {
         const cudaError_t e = cudaStreamQuery(ctx->stream);
@@ -1121,6 +1126,10 @@ struct Solver {
           throw Error(DECO_ERR_INTERNAL, "gmres: an Arnoldi step finished without posting its residual");
         }
         if (e != cudaErrorNotReady) DECO_CUDA(e);
+        const double now = trace_clock_ms();
+        if (t0 < 0.0) t0 = now;
+        else if (now - t0 > step_timeout_ms)
+          throw Error(DECO_ERR_CUDA, "gmres: an Arnoldi step did not finish within DECO_STEP_TIMEOUT seconds");
       }
     }
     std::atomic_thread_fence(std::memory_order_acquire);
