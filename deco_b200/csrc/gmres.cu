@@ -25,6 +25,7 @@
 // the solution update in float64 (iterative refinement).
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <mutex>
@@ -1126,7 +1127,8 @@ struct Solver {
           throw Error(DECO_ERR_INTERNAL, "gmres: an Arnoldi step finished without posting its residual");
         }
         if (e != cudaErrorNotReady) DECO_CUDA(e);
-        const double now = trace_clock_ms();
+        const double now =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
         if (t0 < 0.0) t0 = now;
         else if (now - t0 > step_timeout_ms)
           throw Error(DECO_ERR_CUDA, "gmres: an Arnoldi step did not finish within DECO_STEP_TIMEOUT seconds");
