@@ -504,7 +504,7 @@ __global__ void __launch_bounds__(kThreads) arnoldi_dots_bulk(long long n, long 
     for (int k = 0; k < CPW; ++k) {
       if (k < nk && !dead) {
         issue();  // unit cu + kStages - 1 into the stage unit cu - 1 used
-        // the verdict is made warp-uniform, so the lanes stay converged
+        // the outcome is made warp-uniform, so the lanes stay converged
         if (!__all_sync(0xffffffffu, mbar_wait_bounded(bar + cst, cph))) {
           dead = true;
           if (lane == 0) st.sc[SC_TIMEOUT] = 1.0;
