@@ -30,7 +30,8 @@ __global__ void to_f32(const double* __restrict__ a, float* __restrict__ b, long
 // (each row's columns are ascending, so its block columns are too); bs is a
 // template argument so the divisions by it compile to multiplications
 template <int bs>
-__global__ void bsr_count(int nbr, const int* __restrict__ r, const int* __restrict__ c, int* __restrict__ cnt) {
+__global__ void bsr_count(int nbr, const int* __restrict__ r, const int* __restrict__ c, int* __restrict__ cnt,
+                          unsigned char* __restrict__ full) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nbr; s += gridDim.x * blockDim.x) {
     int pos[3], end[3];
     for (int q = 0; q < bs; ++q) { pos[q] = r[s * bs + q]; end[q] = r[s * bs + q + 1]; }
@@ -45,6 +46,29 @@ __global__ void bsr_count(int nbr, const int* __restrict__ r, const int* __restr
         while (pos[q] < end[q] && c[pos[q]] / bs == mn) ++pos[q];
     }
     cnt[s] = k;
+    // every row of the cell holds all bs entries of each of the k blocks: entry j of
+    // a row is then column j % bs of block j / bs (bsr_fill_rows copies it directly)
+    bool f = true;
+    for (int q = 0; q < bs; ++q) f = f && (r[s * bs + q + 1] - r[s * bs + q] == k * bs);
+    full[s] = f ? 1 : 0;
+  }
+}
+
+// complete cells, one thread per row: entry j of row i goes to column j % bs of
+// the cell's block j / bs (no merge); the other cells are left to bsr_fill
+template <int bs>
+__global__ void bsr_fill_rows(int n, const int* __restrict__ r, const int* __restrict__ c,
+                              const double* __restrict__ v, const int* __restrict__ br,
+                              const unsigned char* __restrict__ full, int* __restrict__ bc, double* __restrict__ bv,
+                              long long plane) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int s = i / bs, q = i % bs;
+    if (!full[s]) continue;
+    const int a = r[i], e = r[i + 1], k0 = br[s];
+    double* __restrict__ dst = bv + q * plane + (long long)k0 * bs;
+    for (int j = 0; j < e - a; ++j) dst[j] = v[a + j];
+    if (q == 0)
+      for (int j = 0; j < e - a; j += bs) bc[k0 + j / bs] = c[a + j] / bs;
   }
 }
 
@@ -52,8 +76,10 @@ __global__ void bsr_count(int nbr, const int* __restrict__ r, const int* __restr
 // (bv is zero-filled beforehand: absent entries stay zero)
 template <int bs>
 __global__ void bsr_fill(int nbr, const int* __restrict__ r, const int* __restrict__ c, const double* __restrict__ v,
-                         const int* __restrict__ br, int* __restrict__ bc, double* __restrict__ bv, long long plane) {
+                         const int* __restrict__ br, const unsigned char* __restrict__ full, int* __restrict__ bc,
+                         double* __restrict__ bv, long long plane) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nbr; s += gridDim.x * blockDim.x) {
+    if (full[s]) continue;  // bsr_fill_rows copies complete cells
     int pos[3], end[3];
     for (int q = 0; q < bs; ++q) { pos[q] = r[s * bs + q]; end[q] = r[s * bs + q + 1]; }
     int k = br[s];
@@ -445,8 +471,9 @@ void make_bsr(deco_ctx_s* ctx, deco_csr_s* A, int bs, double max_fill) {
   const int nbr = A->n / bs;
   DevBuf<int> cnt(nbr + 1, st);
   const int g = grid_for(ctx, nbr, 256);
-  if (bs == 2) bsr_count<2><<<g, 256, 0, st>>>(nbr, A->r.get(), A->c.get(), cnt.get());
-  else bsr_count<3><<<g, 256, 0, st>>>(nbr, A->r.get(), A->c.get(), cnt.get());
+  DevBuf<unsigned char> full(nbr, st);
+  if (bs == 2) bsr_count<2><<<g, 256, 0, st>>>(nbr, A->r.get(), A->c.get(), cnt.get(), full.get());
+  else bsr_count<3><<<g, 256, 0, st>>>(nbr, A->r.get(), A->c.get(), cnt.get(), full.get());
   DECO_CHECK_LAUNCH();
   DevBuf<int> br(nbr + 1, st);
   const long long nblk = exclusive_scan_int(ctx, cnt.get(), br.get(), nbr);
@@ -458,12 +485,20 @@ void make_bsr(deco_ctx_s* ctx, deco_csr_s* A, int bs, double max_fill) {
   A->bplane = plane;
   A->bv.alloc(plane * bs, st);
   A->bv.zero(st);
-  if (bs == 2)
-    bsr_fill<2><<<g, 256, 0, st>>>(nbr, A->r.get(), A->c.get(), A->v.get(), A->br.get(), A->bc.get(), A->bv.get(),
-                                   plane);
-  else
-    bsr_fill<3><<<g, 256, 0, st>>>(nbr, A->r.get(), A->c.get(), A->v.get(), A->br.get(), A->bc.get(), A->bv.get(),
-                                   plane);
+  const int gr = grid_for(ctx, A->n, 256);
+  if (bs == 2) {
+    bsr_fill_rows<2><<<gr, 256, 0, st>>>(A->n, A->r.get(), A->c.get(), A->v.get(), A->br.get(), full.get(),
+                                         A->bc.get(), A->bv.get(), plane);
+    DECO_CHECK_LAUNCH();
+    bsr_fill<2><<<g, 256, 0, st>>>(nbr, A->r.get(), A->c.get(), A->v.get(), A->br.get(), full.get(), A->bc.get(),
+                                   A->bv.get(), plane);
+  } else {
+    bsr_fill_rows<3><<<gr, 256, 0, st>>>(A->n, A->r.get(), A->c.get(), A->v.get(), A->br.get(), full.get(),
+                                         A->bc.get(), A->bv.get(), plane);
+    DECO_CHECK_LAUNCH();
+    bsr_fill<3><<<g, 256, 0, st>>>(nbr, A->r.get(), A->c.get(), A->v.get(), A->br.get(), full.get(), A->bc.get(),
+                                   A->bv.get(), plane);
+  }
   DECO_CHECK_LAUNCH();
   A->bbs = bs;
   A->avg_blk = double(nblk) / nbr;
