@@ -100,215 +100,252 @@ __device__ __forceinline__ void store_at(double* arr, int idx, double val) {
     if (t == idx) arr[t] = val;
 }
 
-template <int BS>  // 2 or 3; 0: the block size from a.bs (at most 3)
-__global__ void cpr_decouple(DecoupleArgs a) {
+// One cell of the decoupling: fix_diag -> weights -> row scaling -> DRS -> IMPES
+// -> CPD in the reference's order.  r, c and v are the matrix's row pointers,
+// columns and values, or a block's staged copy of its cells' rows (row pointers
+// rebased to the copy); b and the per-cell outputs are always global.
+template <int BS>
+__device__ __forceinline__ void decouple_cell(const DecoupleArgs& a, int s, const int* __restrict__ r,
+                                              const int* __restrict__ c, double* __restrict__ v) {
   const int bs = BS > 0 ? BS : a.bs;
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.sn; s += gridDim.x * blockDim.x) {
-    const int* __restrict__ r = a.r;
-    const int* __restrict__ c = a.c;
-    double* __restrict__ v = a.v;
-    double* __restrict__ b = a.b;
-    const int i0 = s * bs;
-    // rows of a cell must share one pattern (IMPES/CPD work position by position)
-    const int len = r[i0 + 1] - r[i0];
-    for (int p = 1; p < bs; ++p)
-      if (r[i0 + p + 1] - r[i0 + p] != len) { atomicExch(a.err, ERR_PATTERN); return; }
+  double* __restrict__ b = a.b;
+  const int i0 = s * bs;
+  // rows of a cell must share one pattern (IMPES/CPD work position by position)
+  const int len = r[i0 + 1] - r[i0];
+  for (int p = 1; p < bs; ++p)
+    if (r[i0 + p + 1] - r[i0 + p] != len) { atomicExch(a.err, ERR_PATTERN); return; }
 
-    // ---- fix_diag (CPR.hpp:753-840), small_tol = big_tol = 1e-20
-    const double tol = 1e-20;
-    unsigned char op = 0;
-    {
-      int j0 = bsearch_le(c, r[i0], r[i0 + 1], i0);
-      if (fabs(v[j0]) < tol) { v[j0] = (v[j0] > 0) ? tol : -tol; a.chk[i0] = 1; atomicAdd(a.nfixed, 1); }
-      if (bs == 3) {
-        int j1 = bsearch_le(c, r[i0 + 1], r[i0 + 2], i0 + 1);
-        int j2 = bsearch_le(c, r[i0 + 2], r[i0 + 3], i0 + 2);
-        if (fabs(v[j1]) < tol || fabs(v[j2]) < tol) {
-          if (fabs(v[j1 + 1]) > tol || fabs(v[j2 - 1]) > tol) {
-            const int ia1 = r[i0 + 1], ib1 = r[i0 + 2];
-            for (int t = 0; t < ib1 - ia1; ++t) { double x = v[ia1 + t]; v[ia1 + t] = v[ib1 + t]; v[ib1 + t] = x; }
-            double x = b[i0 + 1]; b[i0 + 1] = b[i0 + 2]; b[i0 + 2] = x;
-            op |= 8;
-          } else {
-            if (fabs(v[j1]) < tol) { v[j1] = (v[j1] > 0) ? tol : -tol; a.chk[i0 + 1] = 1; atomicAdd(a.nfixed, 1); }
-            if (fabs(v[j2]) < tol) { v[j2] = (v[j2] > 0) ? tol : -tol; a.chk[i0 + 2] = 1; atomicAdd(a.nfixed, 1); }
-          }
-        }
-      } else if (bs == 2) {
-        int j1 = bsearch_le(c, r[i0 + 1], r[i0 + 2], i0 + 1);
-        if (fabs(v[j1]) < tol) { v[j1] = (v[j1] > 0) ? tol : -tol; a.chk[i0 + 1] = 1; atomicAdd(a.nfixed, 1); }
-      }
-    }
-
-    // ---- weights
-    double w[3] = {1.0, 0.0, 0.0};
-    if (a.weights == 2) {  // quasi_IMPES_GE (CPR.hpp:372-447), pressure id 0
-      double Apb[4] = {0, 0, 0, 0}, bp[2] = {0, 0};
-      for (int p = 0; p < bs; ++p) {
-        const int i = i0 + p;
-        const int j = bsearch_le(c, r[i], r[i + 1], i);
-        for (int k = 1; k < bs; ++k) {
-          if (p == 0) bp[k - 1] = -v[j + k - p];
-          else store_at<4>(Apb, (p - 1) * (bs - 1) + c[j + k - p] % bs - 1, v[j + k - p]);
-        }
-      }
-      if (bs == 3) {
-        const double det = dsub(dmul(Apb[0], Apb[3]), dmul(Apb[1], Apb[2]));
-        if (det == 0.0) { atomicExch(a.err, ERR_SINGULAR); return; }
-        const double inv = ddiv(1.0, det);
-        const double q0 = dmul(Apb[3], inv), q1 = dmul(-Apb[1], inv), q2 = dmul(-Apb[2], inv), q3 = dmul(Apb[0], inv);
-        w[1] = dadd(dmul(q0, bp[0]), dmul(q2, bp[1]));
-        w[2] = dadd(dmul(q1, bp[0]), dmul(q3, bp[1]));
-      } else if (bs == 2) {
-        if (Apb[0] == 0.0) { atomicExch(a.err, ERR_SINGULAR); return; }
-        w[1] = ddiv(bp[0], Apb[0]);
-      } else {
-        atomicExch(a.err, ERR_BS);
-        return;
-      }
-    } else if (a.weights == 1) {  // quasi_IMPES (CPR.hpp:322-369): B^T w = e_0
-      double B[9];
-      for (int t = 0; t < 9; ++t) B[t] = 0.0;
-      for (int p = 0; p < bs; ++p) {
-        const int i = i0 + p, ia = r[i], ib = r[i + 1];
-        const int j = bsearch_le(c, ia, ib, i);
-        if (c[j] != i) continue;
-        for (int k = 0; k < bs; ++k) {
-          const int q = j + k - p;
-          if (q < ia || q >= ib) continue;
-          if (c[q] / bs == s) store_at<9>(B, p * bs + c[q] % bs, v[q]);
-        }
-      }
-      w[0] = 0.0; w[1] = 0.0; w[2] = 0.0;
-      w[a.pid] = 1.0;
-      small_lu_solve(bs, B, w);
-    }
-    for (int p = 0; p < bs; ++p) a.w0[i0 + p] = w[p];
-    if (a.weights != 0) {
-      for (int p = 0; p < bs; ++p) {
-        const int i = i0 + p;
-        for (int j = r[i]; j < r[i + 1]; ++j) v[j] = dmul(v[j], w[p]);
-        b[i] = dmul(b[i], w[p]);
-      }
-    }
-
-    // ---- DRS (CPR.hpp:518-600)
-    bool wd[3] = {true, true, true};
-    if (a.use_drs) {
-      for (int p = 0; p < bs; ++p) {
-        const int i = i0 + p, ia = r[i], ib = r[i + 1];
-        const double diag = v[bsearch_le(c, ia, ib, i - p)];
-        double off = -fabs(diag);
-        for (int j = ia; j < ib; ++j) off = dadd(off, (c[j] % bs == 0) ? fabs(v[j]) : 0.0);
-        wd[p] = !(diag < dmul(a.e_dd, off));
-      }
-      if (a.e_ps != 0.0) {
-        const int ia = r[i0], ib = r[i0 + 1];
-        const int jd = bsearch_le(c, ia, ib, i0);
-        const double diag = fabs(v[jd]);
-        double off[3] = {0.0, 0.0, 0.0};
-        for (int j = ia; j < ib; ++j) {
-          if (j == jd) continue;
-          const int q = c[j] % bs;
-#pragma unroll
-          for (int t = 0; t < 3; ++t)
-            if (t == q) off[t] = dadd(off[t], fabs(v[j]));
-        }
-        for (int p = 0; p < bs; ++p) wd[p] = wd[p] && !(off[p] < dmul(a.e_ps, diag));
-      }
-      wd[0] = true;
-      if (a.weights != 0)
-        for (int p = 0; p < bs; ++p)
-          if (!wd[p]) {
-            const int i = i0 + p;
-            const double d = w[p];
-            for (int j = r[i]; j < r[i + 1]; ++j) v[j] = ddiv(v[j], d);
-            b[i] = ddiv(b[i], d);
-            w[p] = 1.0;
-          }
-    }
-    for (int p = 0; p < bs; ++p) a.w[i0 + p] = w[p];
-    for (int p = 0; p < bs; ++p) op |= wd[p] ? (1 << p) : 0;
-    a.ops[s] = op;
-
-    // ---- IMPES (CPR.hpp:450-516): pressure row (offset 0) accumulates the others
-    {
-      const int ia0 = r[i0];
-      for (int k = 0; k < bs; ++k) {
-        const int ia = r[i0 + k], ib = r[i0 + k + 1];
-        if (!a.use_drs) {
-          if (k == 0) continue;
-          for (int j = ia; j < ib; ++j) v[ia0 + (j - ia)] = dadd(v[ia0 + (j - ia)], v[j]);
+  // ---- fix_diag (CPR.hpp:753-840), small_tol = big_tol = 1e-20
+  const double tol = 1e-20;
+  unsigned char op = 0;
+  {
+    int j0 = bsearch_le(c, r[i0], r[i0 + 1], i0);
+    if (fabs(v[j0]) < tol) { v[j0] = (v[j0] > 0) ? tol : -tol; a.chk[i0] = 1; atomicAdd(a.nfixed, 1); }
+    if (bs == 3) {
+      int j1 = bsearch_le(c, r[i0 + 1], r[i0 + 2], i0 + 1);
+      int j2 = bsearch_le(c, r[i0 + 2], r[i0 + 3], i0 + 2);
+      if (fabs(v[j1]) < tol || fabs(v[j2]) < tol) {
+        if (fabs(v[j1 + 1]) > tol || fabs(v[j2 - 1]) > tol) {
+          const int ia1 = r[i0 + 1], ib1 = r[i0 + 2];
+          for (int t = 0; t < ib1 - ia1; ++t) { double x = v[ia1 + t]; v[ia1 + t] = v[ib1 + t]; v[ib1 + t] = x; }
+          double x = b[i0 + 1]; b[i0 + 1] = b[i0 + 2]; b[i0 + 2] = x;
+          op |= 8;
         } else {
-          const double ww = wd[k] ? 1.0 : 0.0;
-          if (k == 0) {
-            for (int j = ia; j < ib; ++j) v[j] = dmul(v[j], ww);
-          } else {
-            for (int j = ia; j < ib; ++j) v[ia0 + (j - ia)] = madd(v[ia0 + (j - ia)], ww, v[j]);
-          }
+          if (fabs(v[j1]) < tol) { v[j1] = (v[j1] > 0) ? tol : -tol; a.chk[i0 + 1] = 1; atomicAdd(a.nfixed, 1); }
+          if (fabs(v[j2]) < tol) { v[j2] = (v[j2] > 0) ? tol : -tol; a.chk[i0 + 2] = 1; atomicAdd(a.nfixed, 1); }
         }
       }
-      double sum = 0.0;
-      for (int j = 0; j < bs; ++j) sum = madd(sum, a.use_drs ? (wd[j] ? 1.0 : 0.0) : 1.0, b[i0 + j]);
-      b[i0] = sum;
+    } else if (bs == 2) {
+      int j1 = bsearch_le(c, r[i0 + 1], r[i0 + 2], i0 + 1);
+      if (fabs(v[j1]) < tol) { v[j1] = (v[j1] > 0) ? tol : -tol; a.chk[i0 + 1] = 1; atomicAdd(a.nfixed, 1); }
     }
+  }
 
-    // ---- CPD (CPR.hpp:603-750): J = diag(D) B^{-1}; rows and b of the cell <- J (.)
-    if (a.cpd) {
-      double B[9], Dp[3], o[9];
-      for (int p = 0; p < bs; ++p) {
-        const int i = i0 + p;
-        const int j = bsearch_le(c, r[i], r[i + 1], i);
-        Dp[p] = v[j];
-        for (int k = 0; k < bs; ++k) store_at<9>(B, p * bs + c[j + k - p] % bs, v[j + k - p]);
+  // ---- weights
+  double w[3] = {1.0, 0.0, 0.0};
+  if (a.weights == 2) {  // quasi_IMPES_GE (CPR.hpp:372-447), pressure id 0
+    double Apb[4] = {0, 0, 0, 0}, bp[2] = {0, 0};
+    for (int p = 0; p < bs; ++p) {
+      const int i = i0 + p;
+      const int j = bsearch_le(c, r[i], r[i + 1], i);
+      for (int k = 1; k < bs; ++k) {
+        if (p == 0) bp[k - 1] = -v[j + k - p];
+        else store_at<4>(Apb, (p - 1) * (bs - 1) + c[j + k - p] % bs - 1, v[j + k - p]);
       }
-      if (bs == 3) {
-        const double c0 = dsub(dmul(B[4], B[8]), dmul(B[5], B[7]));
-        const double c1 = dsub(dmul(B[1], B[8]), dmul(B[2], B[7]));
-        const double c2 = dsub(dmul(B[1], B[5]), dmul(B[2], B[4]));
-        const double det = dadd(dsub(dmul(B[0], c0), dmul(B[3], c1)), dmul(B[6], c2));
-        if (det == 0.0) { atomicExch(a.err, ERR_SINGULAR); return; }
-        const double inv = ddiv(1.0, det);
-        o[0] = dmul(dmul(c0, inv), Dp[0]);
-        o[1] = dmul(dmul(-c1, inv), Dp[0]);
-        o[2] = dmul(dmul(c2, inv), Dp[0]);
-        o[3] = dmul(dmul(-dsub(dmul(B[3], B[8]), dmul(B[5], B[6])), inv), Dp[1]);
-        o[4] = dmul(dmul(dsub(dmul(B[0], B[8]), dmul(B[2], B[6])), inv), Dp[1]);
-        o[5] = dmul(dmul(-dsub(dmul(B[0], B[5]), dmul(B[2], B[3])), inv), Dp[1]);
-        o[6] = dmul(dmul(dsub(dmul(B[3], B[7]), dmul(B[4], B[6])), inv), Dp[2]);
-        o[7] = dmul(dmul(-dsub(dmul(B[0], B[7]), dmul(B[1], B[6])), inv), Dp[2]);
-        o[8] = dmul(dmul(dsub(dmul(B[0], B[4]), dmul(B[1], B[3])), inv), Dp[2]);
-      } else if (bs == 2) {
-        const double det = dsub(dmul(B[0], B[3]), dmul(B[1], B[2]));
-        if (det == 0.0) { atomicExch(a.err, ERR_SINGULAR); return; }
-        const double inv = ddiv(1.0, det);
-        o[0] = dmul(dmul(B[3], inv), Dp[0]);
-        o[1] = dmul(dmul(-B[1], inv), Dp[0]);
-        o[2] = dmul(dmul(-B[2], inv), Dp[1]);
-        o[3] = dmul(dmul(B[0], inv), Dp[1]);
+    }
+    if (bs == 3) {
+      const double det = dsub(dmul(Apb[0], Apb[3]), dmul(Apb[1], Apb[2]));
+      if (det == 0.0) { atomicExch(a.err, ERR_SINGULAR); return; }
+      const double inv = ddiv(1.0, det);
+      const double q0 = dmul(Apb[3], inv), q1 = dmul(-Apb[1], inv), q2 = dmul(-Apb[2], inv), q3 = dmul(Apb[0], inv);
+      w[1] = dadd(dmul(q0, bp[0]), dmul(q2, bp[1]));
+      w[2] = dadd(dmul(q1, bp[0]), dmul(q3, bp[1]));
+    } else if (bs == 2) {
+      if (Apb[0] == 0.0) { atomicExch(a.err, ERR_SINGULAR); return; }
+      w[1] = ddiv(bp[0], Apb[0]);
+    } else {
+      atomicExch(a.err, ERR_BS);
+      return;
+    }
+  } else if (a.weights == 1) {  // quasi_IMPES (CPR.hpp:322-369): B^T w = e_0
+    double B[9];
+    for (int t = 0; t < 9; ++t) B[t] = 0.0;
+    for (int p = 0; p < bs; ++p) {
+      const int i = i0 + p, ia = r[i], ib = r[i + 1];
+      const int j = bsearch_le(c, ia, ib, i);
+      if (c[j] != i) continue;
+      for (int k = 0; k < bs; ++k) {
+        const int q = j + k - p;
+        if (q < ia || q >= ib) continue;
+        if (c[q] / bs == s) store_at<9>(B, p * bs + c[q] % bs, v[q]);
+      }
+    }
+    w[0] = 0.0; w[1] = 0.0; w[2] = 0.0;
+    w[a.pid] = 1.0;
+    small_lu_solve(bs, B, w);
+  }
+  for (int p = 0; p < bs; ++p) a.w0[i0 + p] = w[p];
+  if (a.weights != 0) {
+    for (int p = 0; p < bs; ++p) {
+      const int i = i0 + p;
+      for (int j = r[i]; j < r[i + 1]; ++j) v[j] = dmul(v[j], w[p]);
+      b[i] = dmul(b[i], w[p]);
+    }
+  }
+
+  // ---- DRS (CPR.hpp:518-600)
+  bool wd[3] = {true, true, true};
+  if (a.use_drs) {
+    for (int p = 0; p < bs; ++p) {
+      const int i = i0 + p, ia = r[i], ib = r[i + 1];
+      const double diag = v[bsearch_le(c, ia, ib, i - p)];
+      double off = -fabs(diag);
+      for (int j = ia; j < ib; ++j) off = dadd(off, (c[j] % bs == 0) ? fabs(v[j]) : 0.0);
+      wd[p] = !(diag < dmul(a.e_dd, off));
+    }
+    if (a.e_ps != 0.0) {
+      const int ia = r[i0], ib = r[i0 + 1];
+      const int jd = bsearch_le(c, ia, ib, i0);
+      const double diag = fabs(v[jd]);
+      double off[3] = {0.0, 0.0, 0.0};
+      for (int j = ia; j < ib; ++j) {
+        if (j == jd) continue;
+        const int q = c[j] % bs;
+#pragma unroll
+        for (int t = 0; t < 3; ++t)
+          if (t == q) off[t] = dadd(off[t], fabs(v[j]));
+      }
+      for (int p = 0; p < bs; ++p) wd[p] = wd[p] && !(off[p] < dmul(a.e_ps, diag));
+    }
+    wd[0] = true;
+    if (a.weights != 0)
+      for (int p = 0; p < bs; ++p)
+        if (!wd[p]) {
+          const int i = i0 + p;
+          const double d = w[p];
+          for (int j = r[i]; j < r[i + 1]; ++j) v[j] = ddiv(v[j], d);
+          b[i] = ddiv(b[i], d);
+          w[p] = 1.0;
+        }
+  }
+  for (int p = 0; p < bs; ++p) a.w[i0 + p] = w[p];
+  for (int p = 0; p < bs; ++p) op |= wd[p] ? (1 << p) : 0;
+  a.ops[s] = op;
+
+  // ---- IMPES (CPR.hpp:450-516): pressure row (offset 0) accumulates the others
+  {
+    const int ia0 = r[i0];
+    for (int k = 0; k < bs; ++k) {
+      const int ia = r[i0 + k], ib = r[i0 + k + 1];
+      if (!a.use_drs) {
+        if (k == 0) continue;
+        for (int j = ia; j < ib; ++j) v[ia0 + (j - ia)] = dadd(v[ia0 + (j - ia)], v[j]);
       } else {
-        atomicExch(a.err, ERR_BS);
-        return;
-      }
-      for (int t = 0; t < bs * bs; ++t) a.J[(long long)s * bs * bs + t] = o[t];
-      // position by position: new row p = J[p,p] * row p + sum_{k != p} J[p,k] * row k
-      for (int t = 0; t < len; ++t) {
-        double old[3];
-        for (int k = 0; k < bs; ++k) old[k] = v[r[i0 + k] + t];
-        for (int p = 0; p < bs; ++p) {
-          double nv = dmul(old[p], o[p * bs + p]);
-          for (int k = 0; k < bs; ++k)
-            if (k != p) nv = madd(nv, old[k], o[p * bs + k]);
-          v[r[i0 + p] + t] = nv;
+        const double ww = wd[k] ? 1.0 : 0.0;
+        if (k == 0) {
+          for (int j = ia; j < ib; ++j) v[j] = dmul(v[j], ww);
+        } else {
+          for (int j = ia; j < ib; ++j) v[ia0 + (j - ia)] = madd(v[ia0 + (j - ia)], ww, v[j]);
         }
       }
-      double xb[3], sum[3];
-      for (int k = 0; k < bs; ++k) xb[k] = b[i0 + k];
+    }
+    double sum = 0.0;
+    for (int j = 0; j < bs; ++j) sum = madd(sum, a.use_drs ? (wd[j] ? 1.0 : 0.0) : 1.0, b[i0 + j]);
+    b[i0] = sum;
+  }
+
+  // ---- CPD (CPR.hpp:603-750): J = diag(D) B^{-1}; rows and b of the cell <- J (.)
+  if (a.cpd) {
+    double B[9], Dp[3], o[9];
+    for (int p = 0; p < bs; ++p) {
+      const int i = i0 + p;
+      const int j = bsearch_le(c, r[i], r[i + 1], i);
+      Dp[p] = v[j];
+      for (int k = 0; k < bs; ++k) store_at<9>(B, p * bs + c[j + k - p] % bs, v[j + k - p]);
+    }
+    if (bs == 3) {
+      const double c0 = dsub(dmul(B[4], B[8]), dmul(B[5], B[7]));
+      const double c1 = dsub(dmul(B[1], B[8]), dmul(B[2], B[7]));
+      const double c2 = dsub(dmul(B[1], B[5]), dmul(B[2], B[4]));
+      const double det = dadd(dsub(dmul(B[0], c0), dmul(B[3], c1)), dmul(B[6], c2));
+      if (det == 0.0) { atomicExch(a.err, ERR_SINGULAR); return; }
+      const double inv = ddiv(1.0, det);
+      o[0] = dmul(dmul(c0, inv), Dp[0]);
+      o[1] = dmul(dmul(-c1, inv), Dp[0]);
+      o[2] = dmul(dmul(c2, inv), Dp[0]);
+      o[3] = dmul(dmul(-dsub(dmul(B[3], B[8]), dmul(B[5], B[6])), inv), Dp[1]);
+      o[4] = dmul(dmul(dsub(dmul(B[0], B[8]), dmul(B[2], B[6])), inv), Dp[1]);
+      o[5] = dmul(dmul(-dsub(dmul(B[0], B[5]), dmul(B[2], B[3])), inv), Dp[1]);
+      o[6] = dmul(dmul(dsub(dmul(B[3], B[7]), dmul(B[4], B[6])), inv), Dp[2]);
+      o[7] = dmul(dmul(-dsub(dmul(B[0], B[7]), dmul(B[1], B[6])), inv), Dp[2]);
+      o[8] = dmul(dmul(dsub(dmul(B[0], B[4]), dmul(B[1], B[3])), inv), Dp[2]);
+    } else if (bs == 2) {
+      const double det = dsub(dmul(B[0], B[3]), dmul(B[1], B[2]));
+      if (det == 0.0) { atomicExch(a.err, ERR_SINGULAR); return; }
+      const double inv = ddiv(1.0, det);
+      o[0] = dmul(dmul(B[3], inv), Dp[0]);
+      o[1] = dmul(dmul(-B[1], inv), Dp[0]);
+      o[2] = dmul(dmul(-B[2], inv), Dp[1]);
+      o[3] = dmul(dmul(B[0], inv), Dp[1]);
+    } else {
+      atomicExch(a.err, ERR_BS);
+      return;
+    }
+    for (int t = 0; t < bs * bs; ++t) a.J[(long long)s * bs * bs + t] = o[t];
+    // position by position: new row p = J[p,p] * row p + sum_{k != p} J[p,k] * row k
+    for (int t = 0; t < len; ++t) {
+      double old[3];
+      for (int k = 0; k < bs; ++k) old[k] = v[r[i0 + k] + t];
       for (int p = 0; p < bs; ++p) {
-        sum[p] = 0.0;
-        for (int j = 0; j < bs; ++j) sum[p] = madd(sum[p], o[p * bs + j], xb[j]);
+        double nv = dmul(old[p], o[p * bs + p]);
+        for (int k = 0; k < bs; ++k)
+          if (k != p) nv = madd(nv, old[k], o[p * bs + k]);
+        v[r[i0 + p] + t] = nv;
       }
-      for (int p = 0; p < bs; ++p) b[i0 + p] = sum[p];
+    }
+    double xb[3], sum[3];
+    for (int k = 0; k < bs; ++k) xb[k] = b[i0 + k];
+    for (int p = 0; p < bs; ++p) {
+      sum[p] = 0.0;
+      for (int j = 0; j < bs; ++j) sum[p] = madd(sum[p], o[p * bs + j], xb[j]);
+    }
+    for (int p = 0; p < bs; ++p) b[i0 + p] = sum[p];
+  }
+}
+
+// Cells in groups of blockDim.x: each group's rows (row pointers, columns,
+// values) are first staged in shared memory with coalesced loads, the cells run
+// on the staged copy (their searches and row walks hit shared memory instead of
+// dependent global loads), and the values go back with coalesced stores.  A group
+// whose rows do not fit the staging space runs on global memory.
+template <int BS>  // 2 or 3; 0: the block size from a.bs (at most 3)
+__global__ void cpr_decouple(DecoupleArgs a, int stage_entries) {
+  const int bs = BS > 0 ? BS : a.bs;
+  extern __shared__ __align__(16) unsigned char dsm[];
+  const int nb = blockDim.x;
+  double* vs = reinterpret_cast<double*>(dsm);                 // stage_entries values
+  int* cs = reinterpret_cast<int*>(vs + stage_entries);        // stage_entries columns
+  int* rs = cs + stage_entries;                                 // nb * bs + 1 row pointers
+  for (int base = blockIdx.x * nb; base < a.sn; base += gridDim.x * nb) {
+    const int s = base + threadIdx.x;
+    const int cend = min(base + nb, a.sn);
+    const int row0 = base * bs, row1 = cend * bs;
+    const int e0 = a.r[row0], ne = a.r[row1] - e0;
+    const bool staged = ne <= stage_entries;  // the same for every thread of the block
+    if (staged) {
+      for (int t = threadIdx.x; t <= row1 - row0; t += nb) rs[t] = a.r[row0 + t] - e0;
+      for (int t = threadIdx.x; t < ne; t += nb) {
+        cs[t] = a.c[e0 + t];
+        vs[t] = a.v[e0 + t];
+      }
+      __syncthreads();
+      // row i of the group at rs[i - row0]; its entries at [rs[..], rs[.. + 1]) of cs / vs
+      if (s < a.sn) decouple_cell<BS>(a, s, rs - row0, cs, vs);
+      __syncthreads();
+      for (int t = threadIdx.x; t < ne; t += nb) a.v[e0 + t] = vs[t];
+      __syncthreads();  // the copy is read before the next group overwrites it
+    } else if (s < a.sn) {
+      decouple_cell<BS>(a, s, a.r, a.c, a.v);
     }
   }
 }
@@ -508,9 +545,18 @@ static void cpr_build(deco_ctx_s* ctx, deco_csr_s* A, double* d_b, const deco_cp
   a.e_dd = prm.drs_e_dd; a.e_ps = prm.drs_e_ps;
   a.r = A->r.get(); a.c = A->c.get(); a.v = A->v.get(); a.b = d_b;
   a.w = P->w.get(); a.w0 = P->w0.get(); a.ops = P->ops.get(); a.J = P->J.get(); a.chk = P->check_diag.get(); a.err = flags.get(); a.nfixed = flags.get() + 1;
-  if (bs == 2) cpr_decouple<2><<<grid_for(ctx, P->sn, 128, 16), 128, 0, st>>>(a);
-  else if (bs == 3) cpr_decouple<3><<<grid_for(ctx, P->sn, 128, 16), 128, 0, st>>>(a);
-  else cpr_decouple<0><<<grid_for(ctx, P->sn, 128, 16), 128, 0, st>>>(a);
+  // groups of 128 cells (64 for bs 3) staged in 64 KB of shared memory: 3.6k
+  // entries for a 7-point bs-2 group, about 4.6k for bs 3, room for 5.3k
+  const int nbk = bs == 3 ? 64 : 128;
+  const size_t dsmem = 64 * 1024;
+  const int stage_entries = (int)((dsmem - sizeof(int) * ((size_t)nbk * bs + 1)) / (sizeof(double) + sizeof(int)));
+  auto go = [&](auto kern) {
+    DECO_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
+    kern<<<grid_for(ctx, P->sn, nbk, 16), nbk, dsmem, st>>>(a, stage_entries);
+  };
+  if (bs == 2) go(cpr_decouple<2>);
+  else if (bs == 3) go(cpr_decouple<3>);
+  else go(cpr_decouple<0>);
   DECO_CHECK_LAUNCH();
   int hf[2];
   DECO_CUDA(cudaMemcpyAsync(hf, flags.get(), sizeof(hf), cudaMemcpyDeviceToHost, st));
