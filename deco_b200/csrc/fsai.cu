@@ -11,7 +11,8 @@
 // restatement bit for bit and the reference's LAPACK to rounding.
 //
 // Rows are grouped by order k into classes and processed in ONE launch:
-//   class 1 (k <= 8): one thread per row, M held in registers;
+//   class 1 (k <= 7): one thread per row, M held per thread (registers and
+//            its local frame);
 //   classes 2-3 (k <= 16, <= 32): a group of S = 16 or 32 lanes per row, lane
 //            c holding column c of M in registers; the pivot row's multipliers
 //            travel by shuffles;
@@ -164,7 +165,7 @@ __global__ void __launch_bounds__(kSqWarps * 32) lower_square(int n, const int* 
 
 // ------------------------------------------------------------- row classes
 __device__ __forceinline__ int order_class(int k) {
-  return k <= 0 ? 0 : (k <= 8 ? 1 : (k <= 16 ? 2 : (k <= 32 ? 3 : (k <= 64 ? 4 : 5))));
+  return k <= 0 ? 0 : (k <= 7 ? 1 : (k <= 16 ? 2 : (k <= 32 ? 3 : (k <= 64 ? 4 : 5))));
 }
 
 __global__ void class_hist(int n, const int* __restrict__ fr, int* __restrict__ hist, int* __restrict__ kmax) {
@@ -604,7 +605,7 @@ __device__ __forceinline__ void group_row(int q, int nq, const int* __restrict__
   solve_row_group<S>(q < nq ? rows[q] : -1, gP + g0, gB + g0, gPv + g0, Ar, Ac, Av, Fr, Fc, FLv, FUv);
 }
 
-// KR: the register order of class 1 (4 when no row is wider, 8 otherwise);
+// KR: the order of class 1's per-thread system (4 when no row is wider, else 7);
 // WIDE: whether classes 2-4 occur.  The narrow instantiations carry only the
 // class-1 code, so they need far fewer registers (more rows in flight per SM);
 // the launch still covers every row of the factor.
@@ -859,17 +860,17 @@ void fsai_build(deco_ctx_s* ctx, const deco_csr_s* A0, double tol_rel, double to
     const size_t smem = n4 > 0 ? kSmemBytes : 0;
     const int4 cnt4 = make_int4(n1, n2, n3, n4), off4 = make_int4(0, n1, n1 + n2, n1 + n2 + n3);
     if (n2 + n3 + n4 > 0) {
-      if (smem) DECO_CUDA(cudaFuncSetAttribute(fsai_local_systems<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      if (smem) DECO_CUDA(cudaFuncSetAttribute(fsai_local_systems<7, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                kSmemBytes));
-      fsai_local_systems<8, true><<<nblk, kLuBlock, smem, st>>>(perm.get(), cnt4, off4, b1, b2, b3, A->r.get(),
+      fsai_local_systems<7, true><<<nblk, kLuBlock, smem, st>>>(perm.get(), cnt4, off4, b1, b2, b3, A->r.get(),
                                                                 A->c.get(), A->v.get(), FL.r.get(), FL.c.get(),
                                                                 FL.v.get(), fu.get());
     } else if (h[8] <= 4) {
       fsai_local_systems<4, false><<<nblk, kLuBlock, 0, st>>>(perm.get(), cnt4, off4, b1, b2, b3, A->r.get(),
                                                               A->c.get(), A->v.get(), FL.r.get(), FL.c.get(),
                                                               FL.v.get(), fu.get());
-    } else {
-      fsai_local_systems<8, false><<<nblk, kLuBlock, 0, st>>>(perm.get(), cnt4, off4, b1, b2, b3, A->r.get(),
+    } else {  // orders up to 7 (the 2x2 cells of a 7-point stencil)
+      fsai_local_systems<7, false><<<nblk, kLuBlock, 0, st>>>(perm.get(), cnt4, off4, b1, b2, b3, A->r.get(),
                                                               A->c.get(), A->v.get(), FL.r.get(), FL.c.get(),
                                                               FL.v.get(), fu.get());
     }
