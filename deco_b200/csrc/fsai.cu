@@ -51,28 +51,64 @@ __device__ __forceinline__ bool keep_entry(int i, int col, double v, double D, d
   return (tol_rel == 0.0 || a > D) && (tol_abs == 0.0 || a > tol_abs);
 }
 
+// Half a warp per row: each lane takes every 16th entry, a ballot gives the kept
+// entries' positions, so the row's reads and the compacted writes are coalesced
+// (one thread per row walked its row alone: 2.4 ms for the 111M entries of the
+// 8M-row system).  The kept entries keep their order.
+__device__ __forceinline__ double filter_diag_tol(int i, int a, int e, const int* __restrict__ c,
+                                                  const double* __restrict__ v, double tol_rel, unsigned hmask) {
+  double D = 0.0;
+  if (tol_rel != 0.0 && (threadIdx.x & 15) == 0) D = fabs(__dmul_rn(v[bsearch_le(c, a, e, i)], tol_rel));
+  return __shfl_sync(hmask, D, 0, 16);
+}
+
 __global__ void filter_count(int n, const int* __restrict__ r, const int* __restrict__ c,
                              const double* __restrict__ v, double tol_rel, double tol_abs, int* __restrict__ cnt) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 15;
+  const unsigned hmask = 0xFFFFu << (threadIdx.x & 16);
+  const long long step = ((long long)gridDim.x * blockDim.x) >> 4;
+  for (long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 4; i < n; i += step) {
     const int a = r[i], e = r[i + 1];
-    double D = 0.0;
-    if (tol_rel != 0.0) D = fabs(__dmul_rn(v[bsearch_le(c, a, e, i)], tol_rel));
+    const double D = filter_diag_tol((int)i, a, e, c, v, tol_rel, hmask);
     int k = 0;
-    for (int j = a; j < e; ++j) k += keep_entry(i, c[j], v[j], D, tol_rel, tol_abs);
-    cnt[i] = k;
+    for (int j0 = a; j0 < e; j0 += 16) {
+      const int j = j0 + lane;
+      const bool keep = j < e && keep_entry((int)i, c[j], v[j], D, tol_rel, tol_abs);
+      k += __popc(__ballot_sync(hmask, keep) & hmask);
+    }
+    if (lane == 0) cnt[i] = k;
   }
 }
 
 __global__ void filter_copy(int n, const int* __restrict__ r, const int* __restrict__ c, const double* __restrict__ v,
                             double tol_rel, double tol_abs, const int* __restrict__ ro, int* __restrict__ co,
                             double* __restrict__ vo) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 15;
+  const unsigned hmask = 0xFFFFu << (threadIdx.x & 16);
+  const unsigned below = hmask & ((1u << (threadIdx.x & 31)) - 1u);  // this half's lanes before this one
+  const long long step = ((long long)gridDim.x * blockDim.x) >> 4;
+  for (long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 4; i < n; i += step) {
     const int a = r[i], e = r[i + 1];
-    double D = 0.0;
-    if (tol_rel != 0.0) D = fabs(__dmul_rn(v[bsearch_le(c, a, e, i)], tol_rel));
+    const double D = filter_diag_tol((int)i, a, e, c, v, tol_rel, hmask);
     int o = ro[i];
-    for (int j = a; j < e; ++j)
-      if (keep_entry(i, c[j], v[j], D, tol_rel, tol_abs)) { co[o] = c[j]; vo[o] = v[j]; ++o; }
+    for (int j0 = a; j0 < e; j0 += 16) {
+      const int j = j0 + lane;
+      int cj = 0;
+      double vj = 0.0;
+      bool keep = false;
+      if (j < e) {
+        cj = c[j];
+        vj = v[j];
+        keep = keep_entry((int)i, cj, vj, D, tol_rel, tol_abs);
+      }
+      const unsigned bal = __ballot_sync(hmask, keep);
+      if (keep) {
+        const int pos = o + __popc(bal & below);
+        co[pos] = cj;
+        vo[pos] = vj;
+      }
+      o += __popc(bal & hmask);
+    }
   }
 }
 
