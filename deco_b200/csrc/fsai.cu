@@ -733,9 +733,34 @@ __global__ void col_scatter(int n, const int* __restrict__ r, const int* __restr
 
 // rows of the transpose get their entries in ascending source-row order, the
 // order the reference's sequential scatter produces (CSR.hpp:193-206)
+// (rows of up to kSortReg entries are sorted in registers: loaded once, an
+// unrolled insertion sort on compile-time indices, stored once)
+constexpr int kSortReg = 12;
 __global__ void sort_rows(int n, const int* __restrict__ r, int* __restrict__ c, double* __restrict__ v) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int a = r[i], e = r[i + 1];
+    if (e - a <= kSortReg) {
+      int kc[kSortReg];
+      double kv[kSortReg];
+#pragma unroll
+      for (int t = 0; t < kSortReg; ++t) {
+        kc[t] = a + t < e ? c[a + t] : INT_MAX;
+        kv[t] = a + t < e ? v[a + t] : 0.0;
+      }
+      // insertion sort: the columns are distinct, so the order is the ascending one
+#pragma unroll
+      for (int t = 1; t < kSortReg; ++t)
+#pragma unroll
+        for (int u = t; u > 0; --u)
+          if (kc[u - 1] > kc[u]) {
+            const int tc = kc[u]; kc[u] = kc[u - 1]; kc[u - 1] = tc;
+            const double tv = kv[u]; kv[u] = kv[u - 1]; kv[u - 1] = tv;
+          }
+#pragma unroll
+      for (int t = 0; t < kSortReg; ++t)
+        if (a + t < e) { c[a + t] = kc[t]; v[a + t] = kv[t]; }
+      continue;
+    }
     for (int j = a + 1; j < e; ++j) {
       const int key = c[j];
       const double val = v[j];
