@@ -47,7 +47,7 @@ def test_two_gloo_ranks_share_independent_systems():
     import torch.multiprocessing as mp
     world = 2
     port = _free_port()
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()  # no fork of this multi-threaded process
     out = mgr.dict()
     mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
     (m0, mx0, it0, w0), (m1, mx1, it1, w1) = out[0], out[1]
@@ -115,7 +115,7 @@ def test_two_gloo_ranks_deal_the_batch():
     import torch.multiprocessing as mp
     world = 2
     port = _free_port()
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()  # no fork of this multi-threaded process
     out = mgr.dict()
     mp.spawn(_batch_worker, args=(world, port, out), nprocs=world, join=True)
     (m0, n0, w0, i0), (m1, n1, w1, i1) = out[0], out[1]

@@ -115,7 +115,7 @@ def test_two_gloo_ranks_match_one_rank():
     ref_it = port.Cpr(prec, s.r, s.c, s.v, s.b).solve(sol)["iter"]
     assert abs(it1 - ref_it) <= max(1, 0.1 * ref_it), (it1, ref_it)
     world, port_ = 2, _free_port()
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()  # no fork of this multi-threaded process
     out = mgr.dict()
     mp.spawn(_worker, args=(world, port_, out, prec, sol), nprocs=world, join=True)
     xs = []
