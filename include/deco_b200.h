@@ -4,7 +4,7 @@
  * This is the drop-in boundary for the reference's hot path (amavliut/deco):
  * the reference's C++ classes CSR, FSAI, CPR and SOL (header-only templates,
  * core/CSR.hpp, precond/FSAI/FSAI.hpp, precond/CPR.hpp, solver/SOL.hpp) are
- * re-expressed on the host side as thin C++ classes (deco_b200/host/*.hpp)
+ * re-expressed on the host side as thin C++ classes (deco_b200/host/deco.hpp)
  * that forward to the functions below.  Signatures use plain pointers and
  * sizes only.
  *
